@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the FSS hot path on B200: DCF evaluation at n = 32 over Z_2^32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step): one party's DCF evaluation of 2^24 elements with input width n = 32,
+output ring Z_2^32 (uint32), groupSize 1, keys in the reference byte layout (652 B/element)
+— the plain drop-in DCF configuration. Inputs are seeded synthetic: alpha, beta, x uniform,
+128-bit seeds uniform, maskedX = x + alpha. Keys are generated on the device before timing
+(they are preprocessed material). The 10.9 GB of keys and the 268 MB of seeds exceed the
+126 MB L2, so no flush is needed between steps.
+
+`value` is device-timed throughput (CUDA events on the launch stream, inputs resident);
+`e2e` is the same through the public API with the per-step maskedX copied in from pinned
+host memory and the shares copied back (keys and seeds stay device-resident, as in a
+two-party deployment). With torchrun, every rank evaluates its own 2^24 elements (weak
+scaling, no data-path collective); times are the max over ranks.
+
+`--impl reference` times the reference's own CPU implementation (FastFss_cpu_dcfEval built
+from its sources into oracle/_ref) on a bounded sample with all host threads.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BITS = 32
+ES = 4
+N_ELEMENTS = 1 << 24
+KEY_BYTES_PER_ELEM = 16 * N_BITS + ES * N_BITS + 2 * ES + ES  # 652
+ALGO_BYTES_PER_ELEM = KEY_BYTES_PER_ELEM + 16 + ES + ES  # key + seed + maskedX + share = 676
+# Evaluation work per element: per level one key schedule (40 S-box lookups) and the two
+# child blocks on the input's path (2 x 160 table lookups).
+LOOKUPS_PER_ELEM = N_BITS * (40 + 2 * 160)
+AES_BLOCKS_PER_ELEM = 2 * N_BITS
+AES_KS_PER_ELEM = N_BITS
+METRIC = "DCF eval Gelem/s at n=32 (Z_2^32)"
+UNIT = "Gelem/s"
+CONFIG = {"workload": "plain DCF eval, 2^24 elements, n=32, Z_2^32 (uint32), groupSize 1, one party per step",
+          "elements_per_rank": N_ELEMENTS, "bitWidthIn": N_BITS, "bitWidthOut": N_BITS, "elementSize": ES,
+          "groupSize": 1, "key_layout": "reference (sCW region + per-element vCW/tCW/lastCW)",
+          "l2": "inputs larger than L2 (10.9 GB keys), no flush"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--elements", type=int, default=N_ELEMENTS)
+    ap.add_argument("--cpu-seconds", type=float, default=4.0, help="wall budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    """Samples nvidia-smi during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU reference timing
+# ------------------------------------------------------------------------------------------
+
+def cpu_reference_rate(seconds: float, sample: int = 1 << 18) -> dict:
+    """Times the reference's FastFss_cpu_dcfEval (oracle/_ref) — or, if that library is not
+    built, the oracle restatement — on a `sample`-element batch of the same workload, with all
+    host threads, repeating for about `seconds` of wall time."""
+    from oracle.pyoracle import Oracle, RefCpu
+
+    threads = os.cpu_count() or 1
+    if RefCpu.available():
+        impl, kind = RefCpu(), "reference"
+    else:
+        impl, kind = Oracle(), "port"
+    impl.set_threads(threads)
+    rng = np.random.default_rng(1)
+    a = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    b = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    s0 = rng.integers(0, 256, size=sample * 16, dtype=np.uint8)
+    s1 = rng.integers(0, 256, size=sample * 16, dtype=np.uint8)
+    x = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    key = impl.dcf_keygen(a, b, s0, s1, N_BITS, N_BITS, 1)
+    impl.dcf_eval(x, key, s0, 0, N_BITS, N_BITS, 1)  # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        impl.dcf_eval(x, key, s0, 0, N_BITS, N_BITS, 1)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    rate = sample * reps / el
+    return {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{reps} x FastFss_cpu_dcfEval over {sample} elements (n=32, u32, one party), {el:.2f} s wall"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.pyoracle import Oracle, RefCpu
+
+    threads = os.cpu_count() or 1
+    if RefCpu.available():
+        impl, kind = RefCpu(), "reference"
+    else:
+        impl, kind = Oracle(), "port"
+    impl.set_threads(threads)
+    sample = 1 << 17
+    rng = np.random.default_rng(2)
+    a = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    b = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    s0 = rng.integers(0, 256, size=sample * 16, dtype=np.uint8)
+    s1 = rng.integers(0, 256, size=sample * 16, dtype=np.uint8)
+    x = rng.integers(0, 2**32, size=sample, dtype=np.uint64).astype(np.uint32)
+    key = impl.dcf_keygen(a, b, s0, s1, N_BITS, N_BITS, 1)
+    for _ in range(args.warmup):
+        impl.dcf_eval(x, key, s0, 0, N_BITS, N_BITS, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        impl.dcf_eval(x, key, s0, 0, N_BITS, N_BITS, 1)
+    el = time.perf_counter() - t0
+    value = sample * args.steps / el / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": dict(CONFIG, reference_sample_elements=sample),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"each step = FastFss_cpu_dcfEval over {sample} of the 2^24 elements"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# GPU run
+# ------------------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import fastfunctionsecretsharing_b200 as F
+    from fastfunctionsecretsharing_b200 import _lib
+    from fastfunctionsecretsharing_b200.sharding import max_over_ranks
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    N = args.elements
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    alpha = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    beta = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    seed0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    seed1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    x = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    masked = x + alpha
+    key = torch.empty(0, dtype=torch.uint8, device=dev)
+    F.dcf_key_gen(key, alpha, beta, seed0, seed1, N_BITS, N_BITS, 1)
+    del seed1, x
+    out = torch.empty(0, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    torch.cuda.synchronize(dev)
+
+    def step():
+        F.dcf_eval(out, masked, key, seed0, 0, N_BITS, N_BITS, 1)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t_begin.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    total_ms = t_begin.elapsed_time(t_end)
+    kernel_ms = statistics.mean(s.elapsed_time(e) for s, e in zip(starts, ends))
+    total_ms = max_over_ranks(total_ms, world)
+    kernel_ms = max_over_ranks(kernel_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = N * world * args.steps / (total_ms / 1e3) / 1e9
+
+    # ---- end to end through the public API, host buffers, H2D + D2H per step ----
+    host_x = masked.cpu().pin_memory()
+    host_out = torch.empty(N, dtype=torch.int32).pin_memory()
+    dev_x = torch.empty_like(masked)
+
+    def e2e_step():
+        dev_x.copy_(host_x, non_blocking=True)
+        F.dcf_eval(out, dev_x, key, seed0, 0, N_BITS, N_BITS, 1)
+        host_out.copy_(out.view(-1), non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e_value = N * world * args.steps / (e2e_ms / 1e3) / 1e9
+
+    # ---- correctness of what was timed: party-1 shares reconstruct beta * [maskedX < alpha] ----
+    y1 = torch.empty(0, dtype=torch.int32, device=dev)
+    F.dcf_eval(out, masked, key, seed0, 0, N_BITS, N_BITS, 1)
+    F.dcf_eval(y1, masked, key, seed1_regen(gen_seed=1234 + rank, N=N, dev=dev), 1, N_BITS, N_BITS, 1)
+    lt = (masked.to(torch.int64) & 0xFFFFFFFF) < (alpha.to(torch.int64) & 0xFFFFFFFF)
+    ok = bool(torch.equal((out + y1).view(-1), torch.where(lt, beta, torch.zeros_like(beta))))
+
+    # ---- roofline: measured shared-memory lookup peak ----
+    sink = torch.empty(4 * 512 * 1024, dtype=torch.uint8, device=dev)
+    lk = ctypes.c_ulonglong(0)
+    h = ctypes.c_void_p(stream.cuda_stream)
+    probe = _lib.fn("FastFss_b200_smemLookupProbe")
+    iters = 20000
+    for _ in range(2):
+        probe(sink.data_ptr(), sink.numel(), iters, ctypes.byref(lk), ctypes.byref(h))
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(5):
+        probe(sink.data_ptr(), sink.numel(), iters, ctypes.byref(lk), ctypes.byref(h))
+    p1.record(stream)
+    torch.cuda.synchronize(dev)
+    peak_glookups = lk.value * 5 / (p0.elapsed_time(p1) / 1e3) / 1e9
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    achieved_glookups = LOOKUPS_PER_ELEM * N / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dcf_eval_n32_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    peaks = {}
+    ppath = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(ppath):
+        with open(ppath) as f:
+            peaks = json.load(f)
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_ach = ALGO_BYTES_PER_ELEM * N / (kernel_ms / 1e3) / 1e9
+    ck = clocks.summary()
+    nominal = None
+    if ck.get("sm_mhz"):
+        nominal = FastFssSm(_lib) * 32 * ck["sm_mhz"] * 1e6 / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded uniform alpha, beta, x, 128-bit seeds)", "config": CONFIG,
+        "roofline": {"bound": "smem", "achieved": achieved_glookups, "peak": peak_glookups, "unit": "Glookup/s",
+                     "frac": achieved_glookups / peak_glookups, "traffic": traffic,
+                     "peak_source": "measured on this GPU by FastFss_b200_smemLookupProbe (conflict-free LDS)",
+                     "nominal_peak_at_sampled_clock": nominal,
+                     "algorithmic_lookups_per_element": LOOKUPS_PER_ELEM,
+                     "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_ach / hbm_peak,
+                             "algorithmic_bytes_per_element": ALGO_BYTES_PER_ELEM,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}},
+        "kernel_ms": kernel_ms,
+        "aes_blocks_per_s": AES_BLOCKS_PER_ELEM * N * world / (kernel_ms / 1e3),
+        "aes_key_expansions_per_s": AES_KS_PER_ELEM * N * world / (kernel_ms / 1e3),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * ES, "d2h_bytes_per_step": N * ES,
+                "note": "public API; maskedX in from pinned host memory and shares out per step; keys/seeds resident"},
+        "gpu_launches": args.steps,
+        "clocks": ck,
+        "shares_reconstruct": ok,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_rate(args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def seed1_regen(gen_seed: int, N: int, dev):
+    """Regenerates party 1's seeds exactly as the set-up drew them (same generator order)."""
+    import torch
+
+    gen = torch.Generator(device=dev).manual_seed(gen_seed)
+    torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    return torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+
+
+def FastFssSm(lib) -> int:
+    return int(lib.fn("FastFss_b200_smCount")())
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,320 @@
+// dpf.cu — distributed point function: key generation, evaluation, full-domain evaluation
+// and multi-point evaluation (sm_100a).
+//
+// Reference behaviour: src/impl/dpf.h:172-380 (algorithm), src/kernel/dpf.h (validation and
+// the evalAll / evalMulti index maps), include/FastFss/cuda/dpf.h (ABI). Key layout:
+//   region A  sCW[N][n][16 B]; region B per element: tLCW, tRCW, lastCW[g].
+//
+// The leaf value convert is initialised the way the reference calls it,
+// init(seed, bitWidthOut, groupSize) (src/impl/dpf.h:278,283,375): the per-value byte width
+// is ceil(groupSize / 8) and the AES-CTR threshold is ceil(groupSize / 8) * bitWidthOut > 16.
+// Keys and shares therefore match the reference bit for bit.
+#include <FastFss/cuda/dpf.h>
+#include <FastFss/dpf.h>
+
+#include "fss_device.cuh"
+#include "fss_host.h"
+
+namespace fss {
+
+constexpr int kDpfThreads = 512;
+
+template <typename GE>
+__global__ void __launch_bounds__(kDpfThreads, 1)
+    dpf_keygen_kernel(uint8_t *__restrict__ key, const GE *__restrict__ alpha, const GE *__restrict__ beta,
+                      const uint8_t *__restrict__ seed0, const uint8_t *__restrict__ seed1, uint32_t n, uint32_t bo,
+                      uint32_t g, size_t N)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const size_t bstr = sizeof(GE) * (2 + (size_t)g);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+    {
+        uint8_t *sCWp = key + i * 16 * n;
+        GE      *kb   = reinterpret_cast<GE *>(key + N * 16 * n + i * bstr);
+        uint32_t s0[4], s1[4];
+        load_block_be(seed0 + 16 * i, s0);
+        load_block_be(seed1 + 16 * i, s1);
+        s0[0] &= ~kSeedTBit;
+        s1[0] &= ~kSeedTBit;
+        uint32_t       t0 = 0, t1 = 1;
+        const uint64_t a  = (uint64_t)alpha[i];
+        uint64_t       tl = 0, tr = 0;
+        for (uint32_t lv = 0; lv < n; lv++)
+        {
+            uint32_t G0[2][4], G1[2][4];
+            prg_block(G0[0], 0), prg_block(G0[1], 1), prg_block(G1[0], 0), prg_block(G1[1], 1);
+            aes_encrypt<2>(A, s0, G0);
+            aes_encrypt<2>(A, s1, G1);
+            const uint32_t tL0 = (G0[0][0] >> 24) & 1u, tR0 = (G0[1][0] >> 24) & 1u;
+            const uint32_t tL1 = (G1[0][0] >> 24) & 1u, tR1 = (G1[1][0] >> 24) & 1u;
+            G0[0][0] &= ~kSeedTBit, G0[1][0] &= ~kSeedTBit, G1[0][0] &= ~kSeedTBit, G1[1][0] &= ~kSeedTBit;
+            const uint32_t keep = (uint32_t)((a >> (n - 1 - lv)) & 1u);
+            uint32_t       sCW[4], k0[4], k1[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+            {
+                sCW[c] = keep ? (G0[0][c] ^ G1[0][c]) : (G0[1][c] ^ G1[1][c]);
+                k0[c]  = keep ? G0[1][c] : G0[0][c];
+                k1[c]  = keep ? G1[1][c] : G1[0][c];
+            }
+            store_block_be(sCWp + 16 * lv, sCW);
+            const uint32_t tLCW = tL0 ^ tL1 ^ keep ^ 1u, tRCW = tR0 ^ tR1 ^ keep;
+            tl |= (uint64_t)tLCW << lv;
+            tr |= (uint64_t)tRCW << lv;
+            const uint32_t m0 = 0u - t0, m1 = 0u - t1;
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+            {
+                s0[c] = k0[c] ^ (sCW[c] & m0);
+                s1[c] = k1[c] ^ (sCW[c] & m1);
+            }
+            const uint32_t tcw = keep ? tRCW : tLCW;
+            t0                 = (keep ? tR0 : tL0) ^ (t0 & tcw);
+            t1                 = (keep ? tR1 : tL1) ^ (t1 & tcw);
+        }
+        kb[0] = (GE)tl;
+        kb[1] = (GE)tr;
+        ConvertStream c0, c1;
+        c0.init(s0, bo, g);
+        c1.init(s1, bo, g);
+        for (uint32_t j = 0; j < g; j++)
+        {
+            const uint64_t b = beta ? (uint64_t)beta[i * g + j] : 1u;
+            uint64_t       v = b - c0.value(A, j) + c1.value(A, j);
+            if (t1) v = 0 - v;
+            kb[2 + j] = (GE)v;
+        }
+    }
+}
+
+// Walks one element's tree along x (already reduced mod 2^n) and writes the g outputs.
+template <typename GE>
+__device__ __forceinline__ void dpf_eval_point(const AesLanes &A, GE *o, const uint8_t *sCWp, const GE *kb,
+                                               const uint8_t *seed, uint32_t party, uint32_t n, uint32_t bo,
+                                               uint32_t g, uint64_t x, uint64_t tl, uint64_t tr)
+{
+    uint32_t s[4];
+    load_block_be(seed, s);
+    s[0] &= ~kSeedTBit;
+    uint32_t t = party;
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        uint32_t cw[4];
+        load_block_be(sCWp + 16 * lv, cw);
+        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
+        uint32_t       st[1][4];
+        prg_block(st[0], dir);
+        aes_encrypt<1>(A, s, st);
+        uint32_t       tn = (st[0][0] >> 24) & 1u;
+        const uint32_t m  = 0u - t;
+        st[0][0] &= ~kSeedTBit;
+#pragma unroll
+        for (int c = 0; c < 4; c++) s[c] = st[0][c] ^ (cw[c] & m);
+        tn ^= (uint32_t)(((dir ? tr : tl) >> lv) & 1u) & t;
+        t = tn;
+    }
+    ConvertStream cv;
+    cv.init(s, bo, g);
+    for (uint32_t j = 0; j < g; j++)
+    {
+        const uint64_t v = cv.value(A, j) + (t ? (uint64_t)__ldg(kb + 2 + j) : 0);
+        o[j]             = (GE)(party ? (0 - v) : v);
+    }
+}
+
+// mode 0: plain eval (work = N); mode 1: evalAll (work = N 2^n); mode 2: evalMulti (N P).
+template <typename GE, int MODE>
+__global__ void __launch_bounds__(kDpfThreads, 1)
+    dpf_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                    const uint8_t *__restrict__ seed, const GE *__restrict__ point, uint32_t party, uint32_t n,
+                    uint32_t bo, uint32_t g, size_t N, size_t per, size_t work)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const size_t bstr = sizeof(GE) * (2 + (size_t)g);
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t i  = (MODE == 0) ? w : w / per;
+        const size_t j  = (MODE == 0) ? 0 : w % per;
+        const GE    *kb = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
+        uint64_t     x;
+        GE          *o;
+        if (MODE == 0)
+        {
+            x = (uint64_t)__ldg(maskedX + i);
+            o = out + i * g;
+        }
+        else if (MODE == 1)
+        {
+            // src/kernel/dpf.h:268-275: out index (maskedX - x) mod 2^n holds dpfEval(x).
+            x                   = (uint64_t)j;
+            const size_t target = ((size_t)__ldg(maskedX + i) - j) & (per - 1);
+            o                   = out + (i * per + target) * g;
+        }
+        else
+        {
+            // src/kernel/dpf.h:490-495: point j evaluates at maskedX - point[j] (ring).
+            x = (uint64_t)(GE)((uint64_t)__ldg(maskedX + i) - (uint64_t)__ldg(point + j));
+            o = out + (i * per + j) * g;
+        }
+        x = mod_bits<GE>(x, n);
+        dpf_eval_point<GE>(A, o, key + i * 16 * n, kb, seed + 16 * i, party, n, bo, g, x, (uint64_t)__ldg(kb),
+                           (uint64_t)__ldg(kb + 1));
+    }
+}
+
+static inline size_t dpf_key_bytes(size_t n, size_t g, size_t es, size_t N)
+{
+    return N * (16 * n + es + es + es * g);
+}
+
+static inline size_t dpf_cache_bytes(size_t n, size_t N)
+{
+    return N * 16 * n;
+}
+
+template <typename GE, int MODE>
+static int dpf_launch(void *out, const void *maskedX, const void *key, const void *seed, const void *point,
+                      int partyId, size_t n, size_t bo, size_t g, size_t N, size_t per, void *cudaStreamPtr)
+{
+    const size_t work = (MODE == 0) ? N : N * per;
+    if (work == 0) return FAST_FSS_SUCCESS;
+    cudaStream_t stream = resolve_stream(cudaStreamPtr);
+    auto         kern   = dpf_eval_kernel<GE, MODE>;
+    if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
+    kern<<<grid_for(work, kDpfThreads, 1), kDpfThreads, kAesSmemTotal, stream>>>(
+        (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (const GE *)point,
+        (uint32_t)partyId, (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, per, work);
+    return launch_status();
+}
+
+} // namespace fss
+
+using namespace fss;
+
+// Validation order follows DpfKeyGenTask::check (src/kernel/dpf.h:32-74).
+extern "C" FAST_FSS_API int FastFss_cuda_dpfKeyGen(void *key, size_t keyDataSize, const void *alpha,
+                                                   size_t alphaDataSize, const void *beta, size_t betaDataSize,
+                                                   const void *seed0, size_t seedDataSize0, const void *seed1,
+                                                   size_t seedDataSize1, size_t bitWidthIn, size_t bitWidthOut,
+                                                   size_t groupSize, size_t elementSize, size_t elementNum,
+                                                   void *cudaStreamPtr)
+{
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum;
+        if (!(0 < bitWidthIn && bitWidthIn <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(0 < bitWidthOut && bitWidthOut <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (groupSize == 0) return FAST_FSS_INVALID_GROUP_SIZE_ERROR;
+        if (keyDataSize != dpf_key_bytes(bitWidthIn, groupSize, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (alphaDataSize != N * es) return FAST_FSS_INVALID_ALPHA_DATA_SIZE_ERROR;
+        if (betaDataSize != 0)
+        {
+            if (betaDataSize != N * es * groupSize) return FAST_FSS_INVALID_BETA_DATA_SIZE_ERROR;
+        }
+        else if (groupSize != 1)
+        {
+            return FAST_FSS_INVALID_BETA_DATA_SIZE_ERROR;
+        }
+        if (seedDataSize0 != N * 16 || seedDataSize1 != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (N == 0) return FAST_FSS_SUCCESS;
+        cudaStream_t stream = resolve_stream(cudaStreamPtr);
+        auto         kern   = dpf_keygen_kernel<GE>;
+        if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
+        kern<<<grid_for(N, kDpfThreads, 1), kDpfThreads, kAesSmemTotal, stream>>>(
+            (uint8_t *)key, (const GE *)alpha, (const GE *)beta, (const uint8_t *)seed0, (const uint8_t *)seed1,
+            (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, (uint32_t)groupSize, N);
+        return launch_status();
+    });
+}
+
+// Validation order follows DpfEvalTask::check (src/kernel/dpf.h:115-160).
+extern "C" FAST_FSS_API int FastFss_cuda_dpfEval(void *sharedOut, size_t sharedOutDataSize, const void *maskedX,
+                                                 size_t maskedXDataSize, const void *key, size_t keyDataSize,
+                                                 const void *seed, size_t seedDataSize, int partyId,
+                                                 size_t bitWidthIn, size_t bitWidthOut, size_t groupSize,
+                                                 size_t elementSize, size_t elementNum, void *cache,
+                                                 size_t cacheDataSize, void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum;
+        if (!(0 < bitWidthIn && bitWidthIn <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(0 < bitWidthOut && bitWidthOut <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (groupSize == 0) return FAST_FSS_INVALID_GROUP_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (keyDataSize != dpf_key_bytes(bitWidthIn, groupSize, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (sharedOutDataSize != N * es * groupSize) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (cacheDataSize != 0 && cacheDataSize != dpf_cache_bytes(bitWidthIn, N))
+            return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+        return dpf_launch<GE, 0>(sharedOut, maskedX, key, seed, nullptr, partyId, bitWidthIn, bitWidthOut, groupSize,
+                                 N, 1, cudaStreamPtr);
+    });
+}
+
+// Validation order follows DpfEvalAllTask::check (src/kernel/dpf.h:203-251).
+extern "C" FAST_FSS_API int FastFss_cuda_dpfEvalAll(void *sharedOut, size_t sharedOutDataSize, const void *maskedX,
+                                                    size_t maskedXDataSize, const void *key, size_t keyDataSize,
+                                                    const void *seed, size_t seedDataSize, int partyId,
+                                                    size_t bitWidthIn, size_t bitWidthOut, size_t groupSize,
+                                                    size_t elementSize, size_t elementNum, void *cache,
+                                                    size_t cacheDataSize, void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum;
+        if (!(0 < bitWidthIn && bitWidthIn <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(0 < bitWidthOut && bitWidthOut <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (groupSize == 0) return FAST_FSS_INVALID_GROUP_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (keyDataSize != dpf_key_bytes(bitWidthIn, groupSize, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        // The full domain must be addressable: the reference computes 1ULL << n here.
+        if (bitWidthIn >= 64) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        const size_t dom = (size_t)1 << bitWidthIn;
+        if (sharedOutDataSize != N * es * dom * groupSize) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (cacheDataSize != 0 && cacheDataSize != dpf_cache_bytes(bitWidthIn, N))
+            return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+        return dpf_launch<GE, 1>(sharedOut, maskedX, key, seed, nullptr, partyId, bitWidthIn, bitWidthOut, groupSize,
+                                 N, dom, cudaStreamPtr);
+    });
+}
+
+// Validation order follows DpfEvalMultiTask::check (src/kernel/dpf.h:406-458).
+extern "C" FAST_FSS_API int FastFss_cuda_dpfEvalMulti(void *sharedOut, size_t sharedOutDataSize, const void *maskedX,
+                                                      size_t maskedXDataSize, const void *key, size_t keyDataSize,
+                                                      const void *seed, size_t seedDataSize, int partyId,
+                                                      const void *point, size_t pointDataSize, size_t bitWidthIn,
+                                                      size_t bitWidthOut, size_t groupSize, size_t elementSize,
+                                                      size_t elementNum, void *cache, size_t cacheDataSize,
+                                                      void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum;
+        if (!(0 < bitWidthIn && bitWidthIn <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(0 < bitWidthOut && bitWidthOut <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (groupSize == 0) return FAST_FSS_INVALID_GROUP_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (pointDataSize % es != 0) return FAST_FSS_INVALID_POINT_DATA_SIZE_ERROR;
+        if (keyDataSize != dpf_key_bytes(bitWidthIn, groupSize, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        const size_t P = pointDataSize / es;
+        if (sharedOutDataSize != N * es * P * groupSize) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (cacheDataSize != 0 && cacheDataSize != dpf_cache_bytes(bitWidthIn, N))
+            return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+        return dpf_launch<GE, 2>(sharedOut, maskedX, key, seed, point, partyId, bitWidthIn, bitWidthOut, groupSize,
+                                 N, P, cudaStreamPtr);
+    });
+}

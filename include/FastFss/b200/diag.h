@@ -1,0 +1,30 @@
+/* Diagnostics of this library (no counterpart in the reference).
+ *
+ * FastFss_b200_smemLookupProbe measures the sustained rate of conflict-free, byte-permute
+ * addressed 32-bit shared-memory table lookups — the access the AES T-table rounds of every
+ * FSS kernel are built from — so a benchmark can report kernel throughput as a fraction of
+ * a measured peak. It launches one 512-thread CTA per SM; each thread runs 8 independent
+ * lookup chains for `iterations` steps and stores one word per thread into `sink`
+ * (sinkBytes >= 4 * 512 * SM count). *lookups receives the total number of lookups issued.
+ * Asynchronous on *(cudaStream_t *)cudaStreamPtr (cudaStreamPerThread when NULL). */
+#ifndef FAST_FSS_B200_DIAG_H
+#define FAST_FSS_B200_DIAG_H
+
+#include <FastFss/api.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+FAST_FSS_API int FastFss_b200_smemLookupProbe(void *sink, size_t sinkBytes, unsigned iterations,
+                                              unsigned long long *lookups, void *cudaStreamPtr);
+
+FAST_FSS_API int FastFss_b200_smCount(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
