@@ -1,0 +1,229 @@
+// dcf_core.cuh — per-element DCF routines shared by the DCF, DCF-MIC and spline kernels.
+//
+// Algorithm: src/impl/dcf.h:187-491 of the reference. Key layout (dcfKeySetPtr,
+// src/impl/dcf.h:139-167): region A sCW[N][n][16 B]; region B per element, stride
+// es (n g + 2 + g): vCW[n][g], tLCW, tRCW, lastCW[g].
+#pragma once
+
+#include "fss_device.cuh"
+
+namespace fss {
+
+template <typename GE>
+struct DcfKeyView
+{
+    const uint8_t *sCW;  // n x 16 B
+    const GE      *vCW;  // n x g
+    uint64_t       tl, tr;
+    const GE      *last; // g
+
+    __device__ __forceinline__ void set(const uint8_t *key, uint32_t n, uint32_t g, size_t i, size_t N)
+    {
+        const size_t bstr = sizeof(GE) * ((size_t)n * g + 2 + g);
+        sCW               = key + i * 16 * n;
+        vCW               = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
+        tl                = (uint64_t)__ldg(vCW + (size_t)n * g);
+        tr                = (uint64_t)__ldg(vCW + (size_t)n * g + 1);
+        last              = vCW + (size_t)n * g + 2;
+    }
+};
+
+// One level of the evaluation walk: expands the child on direction `dir` of node (s, t)
+// (blocks 2 dir and 2 dir + 1 of G(s)), applies the correction word, and leaves the
+// child's seed in s, its control bit in the return value and its value block in v.
+__device__ __forceinline__ uint32_t dcf_step(const AesLanes &A, uint32_t s[4], uint32_t t, uint32_t dir,
+                                             const uint8_t *cwp, uint64_t tl, uint64_t tr, uint32_t lv, uint32_t v[4])
+{
+    uint32_t cw[4];
+    load_block_be(cwp, cw);
+    uint32_t st[2][4];
+    prg_block(st[0], 2 * dir);
+    prg_block(st[1], 2 * dir + 1);
+    aes_encrypt<2>(A, s, st);
+    uint32_t       tn = (st[0][0] >> 24) & 1u;
+    const uint32_t m  = 0u - t;
+    st[0][0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+    {
+        s[c] = st[0][c] ^ (cw[c] & m);
+        v[c] = st[1][c];
+    }
+    tn ^= (uint32_t)(((dir ? tr : tl) >> lv) & 1u) & t;
+    return tn;
+}
+
+// Share of output value `j` only (the group is read out of the convert stream without
+// materialising the other values): used where a caller consumes a slice of the group.
+// out[k] += share of value j0 + k, k < cnt (cnt <= MAXC).
+template <typename GE, int MAXC>
+__device__ __forceinline__ void dcf_eval_slice(const AesLanes &A, uint64_t out[MAXC], const DcfKeyView<GE> &K,
+                                               const uint8_t *seed, uint32_t party, uint32_t n, uint32_t bo,
+                                               uint32_t g, uint64_t x, uint32_t j0, uint32_t cnt)
+{
+    uint32_t s[4];
+    load_block_be(seed, s);
+    s[0] &= ~kSeedTBit;
+    uint32_t t = party;
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
+        uint32_t       v[4];
+        const uint32_t tp = t;
+        t                 = dcf_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv, v);
+        ConvertStream cv;
+        cv.init(v, g, bo);
+#pragma unroll
+        for (int k = 0; k < MAXC; k++)
+        {
+            if ((uint32_t)k < cnt)
+            {
+                const uint64_t val = cv.value(A, j0 + k) + (tp ? (uint64_t)__ldg(K.vCW + (size_t)lv * g + j0 + k) : 0);
+                out[k] += party ? (0 - val) : val;
+            }
+        }
+    }
+    ConvertStream cv;
+    cv.init(s, g, bo);
+#pragma unroll
+    for (int k = 0; k < MAXC; k++)
+    {
+        if ((uint32_t)k < cnt)
+        {
+            const uint64_t val = cv.value(A, j0 + k) + (t ? (uint64_t)__ldg(K.last + j0 + k) : 0);
+            out[k] += party ? (0 - val) : val;
+        }
+    }
+}
+
+// groupSize 1 share (the convert is a plain read of the first ceil(bo/8) bytes).
+template <typename GE>
+__device__ __forceinline__ uint64_t dcf_eval_g1(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
+                                                uint32_t party, uint32_t n, uint32_t bo, uint64_t x)
+{
+    const int ges = (int)((bo + 7) / 8);
+    uint32_t  s[4];
+    load_block_be(seed, s);
+    s[0] &= ~kSeedTBit;
+    uint32_t t   = party;
+    uint64_t acc = 0;
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
+        const uint64_t vcw = (uint64_t)__ldg(K.vCW + lv);
+        uint32_t       v[4];
+        const uint32_t tp = t;
+        t                 = dcf_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv, v);
+        const uint64_t val = block_le_prefix(v, ges) + (tp ? vcw : 0);
+        acc += party ? (0 - val) : val;
+    }
+    const uint64_t val = block_le_prefix(s, ges) + (t ? (uint64_t)__ldg(K.last) : 0);
+    acc += party ? (0 - val) : val;
+    return acc;
+}
+
+// Key generation of one element (src/impl/dcf.h:187-368). beta == nullptr means beta = 1
+// (first value; the reference reads only that one for groupSize 1). vAlpha accumulates in
+// the element's lastCW slots, as in the reference.
+template <typename GE>
+__device__ __forceinline__ void dcf_keygen_element(const AesLanes &A, uint8_t *key, size_t N, size_t i,
+                                                   uint64_t alpha, const GE *beta, const uint8_t *seed0,
+                                                   const uint8_t *seed1, uint32_t n, uint32_t bo, uint32_t g)
+{
+    const size_t bstr = sizeof(GE) * ((size_t)n * g + 2 + g);
+    uint8_t     *sCWp = key + i * 16 * n;
+    GE          *vCW  = reinterpret_cast<GE *>(key + N * 16 * n + i * bstr);
+    GE          *tLp  = vCW + (size_t)n * g;
+    GE          *last = tLp + 2;
+    for (uint32_t j = 0; j < g; j++) last[j] = 0;
+
+    uint32_t s0[4], s1[4];
+    load_block_be(seed0, s0);
+    load_block_be(seed1, s1);
+    s0[0] &= ~kSeedTBit;
+    s1[0] &= ~kSeedTBit;
+    uint32_t t0 = 0, t1 = 1;
+    uint64_t tl = 0, tr = 0;
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        uint32_t G0[4][4], G1[4][4];
+#pragma unroll
+        for (int b = 0; b < 4; b++) prg_block(G0[b], b), prg_block(G1[b], b);
+        aes_encrypt<4>(A, s0, G0);
+        aes_encrypt<4>(A, s1, G1);
+        const uint32_t tL0 = (G0[0][0] >> 24) & 1u, tR0 = (G0[2][0] >> 24) & 1u;
+        const uint32_t tL1 = (G1[0][0] >> 24) & 1u, tR1 = (G1[2][0] >> 24) & 1u;
+        G0[0][0] &= ~kSeedTBit, G0[2][0] &= ~kSeedTBit, G1[0][0] &= ~kSeedTBit, G1[2][0] &= ~kSeedTBit;
+
+        const uint32_t keep = (uint32_t)((alpha >> (n - 1 - lv)) & 1u);
+        // keep = R (1): lose = L = blocks 0/1, keep = blocks 2/3; keep = L (0): the reverse.
+        uint32_t sLose0[4], sLose1[4], vLose0[4], vLose1[4], sKeep0[4], sKeep1[4], vKeep0[4], vKeep1[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+        {
+            sLose0[c] = keep ? G0[0][c] : G0[2][c];
+            vLose0[c] = keep ? G0[1][c] : G0[3][c];
+            sKeep0[c] = keep ? G0[2][c] : G0[0][c];
+            vKeep0[c] = keep ? G0[3][c] : G0[1][c];
+            sLose1[c] = keep ? G1[0][c] : G1[2][c];
+            vLose1[c] = keep ? G1[1][c] : G1[3][c];
+            sKeep1[c] = keep ? G1[2][c] : G1[0][c];
+            vKeep1[c] = keep ? G1[3][c] : G1[1][c];
+        }
+        uint32_t sCW[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) sCW[c] = sLose0[c] ^ sLose1[c];
+
+        ConvertStream cL1, cL0, cK1, cK0;
+        cL1.init(vLose1, g, bo);
+        cL0.init(vLose0, g, bo);
+        cK1.init(vKeep1, g, bo);
+        cK0.init(vKeep0, g, bo);
+        for (uint32_t j = 0; j < g; j++)
+        {
+            uint64_t va = (uint64_t)last[j];
+            uint64_t v  = cL1.value(A, j) - cL0.value(A, j) - va;
+            if (t1) v = 0 - v;
+            if (keep)
+            {
+                const uint64_t b = beta ? (uint64_t)beta[j] : (uint64_t)(j == 0);
+                v += t1 ? (0 - b) : b;
+            }
+            vCW[(size_t)lv * g + j] = (GE)v;
+            va                      = va - cK1.value(A, j) + cK0.value(A, j) + (t1 ? (0 - v) : v);
+            last[j]                 = (GE)va;
+        }
+
+        store_block_be(sCWp + 16 * lv, sCW);
+        const uint32_t tLCW = tL0 ^ tL1 ^ keep ^ 1u;
+        const uint32_t tRCW = tR0 ^ tR1 ^ keep;
+        tl |= (uint64_t)tLCW << lv;
+        tr |= (uint64_t)tRCW << lv;
+        const uint32_t m0 = 0u - t0, m1 = 0u - t1;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+        {
+            s0[c] = sKeep0[c] ^ (sCW[c] & m0);
+            s1[c] = sKeep1[c] ^ (sCW[c] & m1);
+        }
+        const uint32_t tcw = keep ? tRCW : tLCW;
+        t0                 = (keep ? tR0 : tL0) ^ (t0 & tcw);
+        t1                 = (keep ? tR1 : tL1) ^ (t1 & tcw);
+    }
+    tLp[0] = (GE)tl;
+    tLp[1] = (GE)tr;
+    ConvertStream c1, c0;
+    c1.init(s1, g, bo);
+    c0.init(s0, g, bo);
+    for (uint32_t j = 0; j < g; j++)
+    {
+        uint64_t v = c1.value(A, j) - c0.value(A, j) - (uint64_t)last[j];
+        if (t1) v = 0 - v;
+        last[j] = (GE)v;
+    }
+}
+
+} // namespace fss

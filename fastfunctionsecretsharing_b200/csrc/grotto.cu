@@ -1,0 +1,623 @@
+// grotto.cu — Grotto (a Z_2 DPF with 64-bit leaves): key generation, equality and prefix-
+// parity comparison shares, multiple-interval containment, interval lookup tables, and a
+// full-domain expansion (sm_100a).
+//
+// Reference behaviour: src/impl/grotto.h:111-545 (algorithm), src/kernel/grotto.h
+// (validation), include/FastFss/cuda/grotto.h (ABI). Key layout (grottoKeySetPtr,
+// src/impl/grotto.h:53-79): region A sCW[N][n-6][16 B]; region B lastCW[N] (uint64);
+// region C per element tLCW, tRCW (ring elements).
+//
+// Per-party comparison share (grottoEval, src/impl/grotto.h:284-391): parity of the
+// control-bit changes (t_parent ^ t_child) on the right turns of the path, xor the parity of
+// the leaf word below the input's offset, xor the party id. With equalBound the reference
+// returns early once the remaining input bits are zero; every later turn is a left turn and
+// the leaf offset is 0, so the early value equals the full walk's — the full-domain kernel
+// below relies on that to read every x out of one leaf word and one path parity.
+#include <FastFss/b200/grotto_all.h>
+#include <FastFss/cuda/grotto.h>
+#include <FastFss/grotto.h>
+
+#include "fss_device.cuh"
+#include "fss_host.h"
+
+namespace fss {
+
+constexpr int kGrottoThreads = 512;
+
+template <typename GE>
+struct GrottoKeyView
+{
+    const uint8_t *sCW;
+    uint64_t       last, tl, tr;
+
+    __device__ __forceinline__ void set(const uint8_t *key, uint32_t n, size_t i, size_t N)
+    {
+        const size_t a = N * 16 * (n - 6);
+        sCW            = key + i * 16 * (n - 6);
+        last           = __ldg(reinterpret_cast<const unsigned long long *>(key + a) + i);
+        const GE *t    = reinterpret_cast<const GE *>(key + a + N * 8) + 2 * i;
+        tl             = (uint64_t)__ldg(t);
+        tr             = (uint64_t)__ldg(t + 1);
+    }
+};
+
+// Bytes 8..15 of a block (big-endian words 2, 3) as the little-endian uint64 seed[1].
+__device__ __forceinline__ uint64_t hi_u64(const uint32_t w[4])
+{
+    return (uint64_t)bswap32(w[2]) | ((uint64_t)bswap32(w[3]) << 32);
+}
+
+// Expands child `dir` of (s, t) at level lv; returns the child's control bit.
+__device__ __forceinline__ uint32_t grotto_step(const AesLanes &A, uint32_t s[4], uint32_t t, uint32_t dir,
+                                                const uint8_t *cwp, uint64_t tl, uint64_t tr, uint32_t lv)
+{
+    uint32_t cw[4];
+    load_block_be(cwp, cw);
+    uint32_t st[1][4];
+    prg_block(st[0], dir);
+    aes_encrypt<1>(A, s, st);
+    uint32_t       tn = (st[0][0] >> 24) & 1u;
+    const uint32_t m  = 0u - t;
+    st[0][0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++) s[c] = st[0][c] ^ (cw[c] & m);
+    tn ^= (uint32_t)(((dir ? tr : tl) >> lv) & 1u) & t;
+    return tn;
+}
+
+// Root-to-leaf walk along x (x < 2^n). Returns the leaf word u; *parity gets the right-turn
+// parity. With equalBound the walk stops as soon as the remaining bits of x are zero
+// (*early = 1, u undefined).
+template <typename GE>
+__device__ __forceinline__ uint64_t grotto_walk(const AesLanes &A, const GrottoKeyView<GE> &K, const uint8_t *seed,
+                                                uint32_t party, uint32_t n, uint64_t x, bool equalBound,
+                                                uint32_t *parity, bool *early)
+{
+    uint32_t s[4];
+    load_block_be(seed, s);
+    s[0] &= ~kSeedTBit;
+    uint32_t t = party, par = 0;
+    *early     = false;
+#pragma unroll 1
+    for (uint32_t lv = 0; lv + 6 < n; lv++)
+    {
+        if (equalBound && mod_bits<GE>(x, n - lv) == 0)
+        {
+            *early  = true;
+            *parity = par;
+            return 0;
+        }
+        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
+        const uint32_t tn  = grotto_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv);
+        par ^= dir & (t ^ tn);
+        t = tn;
+    }
+    *parity = par;
+    const uint64_t u = hi_u64(s);
+    return t ? (u ^ K.last) : u;
+}
+
+// grottoEval share (src/impl/grotto.h:284-391).
+template <typename GE>
+__device__ __forceinline__ uint32_t grotto_cmp(const AesLanes &A, const GrottoKeyView<GE> &K, const uint8_t *seed,
+                                               uint32_t party, uint32_t n, uint64_t x, bool equalBound)
+{
+    uint32_t       par;
+    bool           early;
+    const uint64_t u = grotto_walk<GE>(A, K, seed, party, n, x, equalBound, &par, &early);
+    if (early) return par ^ party;
+    const uint32_t pre = (uint32_t)(x & 63u);
+    uint64_t       mask;
+    if (equalBound)
+        mask = pre ? (~0ull >> (64 - pre)) : 0ull;
+    else
+        mask = ~0ull >> (63 - pre);
+    return par ^ (uint32_t)(__popcll(u & mask) & 1) ^ party;
+}
+
+// ---------------------------------------------------------------------------------------
+// Key generation (src/impl/grotto.h:111-205)
+// ---------------------------------------------------------------------------------------
+template <typename GE>
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_keygen_kernel(uint8_t *__restrict__ key, const GE *__restrict__ alpha, const uint8_t *__restrict__ seed0,
+                         const uint8_t *__restrict__ seed1, uint32_t n, size_t N)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const size_t a = N * 16 * (n - 6);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+    {
+        uint8_t       *sCWp = key + i * 16 * (n - 6);
+        const uint64_t al   = (uint64_t)alpha[i];
+        uint32_t       s0[4], s1[4];
+        load_block_be(seed0 + 16 * i, s0);
+        load_block_be(seed1 + 16 * i, s1);
+        s0[0] &= ~kSeedTBit;
+        s1[0] &= ~kSeedTBit;
+        uint32_t t0 = 0, t1 = 1;
+        uint64_t tl = 0, tr = 0;
+#pragma unroll 1
+        for (uint32_t lv = 0; lv + 6 < n; lv++)
+        {
+            uint32_t G0[2][4], G1[2][4];
+            prg_block(G0[0], 0), prg_block(G0[1], 1), prg_block(G1[0], 0), prg_block(G1[1], 1);
+            aes_encrypt<2>(A, s0, G0);
+            aes_encrypt<2>(A, s1, G1);
+            const uint32_t tL0 = (G0[0][0] >> 24) & 1u, tR0 = (G0[1][0] >> 24) & 1u;
+            const uint32_t tL1 = (G1[0][0] >> 24) & 1u, tR1 = (G1[1][0] >> 24) & 1u;
+            G0[0][0] &= ~kSeedTBit, G0[1][0] &= ~kSeedTBit, G1[0][0] &= ~kSeedTBit, G1[1][0] &= ~kSeedTBit;
+            const uint32_t keep = (uint32_t)((al >> (n - 1 - lv)) & 1u), lose = 1u - keep;
+            uint32_t       cw[4], k0[4], k1[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+            {
+                cw[c] = lose == 0 ? (G0[0][c] ^ G1[0][c]) : (G0[1][c] ^ G1[1][c]);
+                k0[c] = keep == 0 ? G0[0][c] : G0[1][c];
+                k1[c] = keep == 0 ? G1[0][c] : G1[1][c];
+            }
+            store_block_be(sCWp + 16 * lv, cw);
+            const uint32_t tLCW = tL0 ^ tL1 ^ lose, tRCW = tR0 ^ tR1 ^ keep;
+            tl |= (uint64_t)tLCW << lv;
+            tr |= (uint64_t)tRCW << lv;
+            const uint32_t m0 = 0u - t0, m1 = 0u - t1;
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+            {
+                s0[c] = k0[c] ^ (cw[c] & m0);
+                s1[c] = k1[c] ^ (cw[c] & m1);
+            }
+            const uint32_t tcw = keep ? tRCW : tLCW;
+            t0                 = (keep ? tR0 : tL0) ^ (t0 & tcw);
+            t1                 = (keep ? tR1 : tL1) ^ (t1 & tcw);
+        }
+        reinterpret_cast<unsigned long long *>(key + a)[i] = hi_u64(s0) ^ hi_u64(s1) ^ (1ull << (al & 63u));
+        GE *t                                               = reinterpret_cast<GE *>(key + a + N * 8) + 2 * i;
+        t[0]                                                = (GE)tl;
+        t[1]                                                = (GE)tr;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Point evaluations: mode 0 = equality share, 1 = comparison share (equalBound flag)
+// ---------------------------------------------------------------------------------------
+template <typename GE, int MODE>
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                       const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, bool equalBound, size_t N)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+    {
+        GrottoKeyView<GE> K;
+        K.set(key, n, i, N);
+        const uint64_t x = mod_bits<GE>((uint64_t)__ldg(maskedX + i), n);
+        if (MODE == 0)
+        {
+            uint32_t       par;
+            bool           early;
+            const uint64_t u = grotto_walk<GE>(A, K, seed + 16 * i, party, n, x, false, &par, &early);
+            out[i]           = (GE)((u >> (x & 63u)) & 1u);
+        }
+        else
+        {
+            out[i] = (GE)grotto_cmp<GE>(A, K, seed + 16 * i, party, n, x, equalBound);
+        }
+    }
+}
+
+// Interval endpoints shared by MIC and the LUT (src/impl/grotto.h:414-423,499-517):
+// sp = share of [x - (L - 1) <= alpha'], sq = share of [x - R <= alpha'], bit = sp ^ sq ^
+// party [xQ >= xP] (the reference reuses sq of interval i-1 as sp of interval i when the
+// intervals touch; that point is the same, so every interval is evaluated on its own here).
+template <typename GE>
+__device__ __forceinline__ uint32_t grotto_interval_bit(const AesLanes &A, const GrottoKeyView<GE> &K,
+                                                        const uint8_t *seed, uint32_t party, uint32_t n, uint64_t mx,
+                                                        uint64_t L, uint64_t R)
+{
+    const uint64_t xP = mod_bits<GE>((uint64_t)(GE)(mx - (uint64_t)(GE)(L - 1)), n);
+    const uint64_t xQ = mod_bits<GE>((uint64_t)(GE)(mx - R), n);
+    const uint32_t sp = grotto_cmp<GE>(A, K, seed, party, n, xP, true);
+    const uint32_t sq = grotto_cmp<GE>(A, K, seed, party, n, xQ, true);
+    return (sp ^ sq ^ ((xQ >= xP) ? party : 0u)) & 1u;
+}
+
+// MIC: one thread per (element, interval).
+template <typename GE>
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_mic_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                      const uint8_t *__restrict__ seed, uint32_t party, const GE *__restrict__ left,
+                      const GE *__restrict__ right, uint32_t m, uint32_t n, size_t N)
+{
+    aes_tables_build();
+    AesLanes     A;
+    const size_t work = N * m;
+    A.init();
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t   i = w / m, q = w % m;
+        GrottoKeyView<GE> K;
+        K.set(key, n, i, N);
+        out[w] = (GE)grotto_interval_bit<GE>(A, K, seed + 16 * i, party, n, (uint64_t)__ldg(maskedX + i),
+                                             (uint64_t)__ldg(left + q), (uint64_t)__ldg(right + q));
+    }
+}
+
+// Interval LUT (src/impl/grotto.h:449-545): G lanes per element stride over the intervals;
+// E and T[j0 .. j0 + LMAX) are summed in the ring and reduced with warp shuffles.
+template <typename GE, int LMAX>
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_lut_kernel(GE *__restrict__ outE, GE *__restrict__ outT, const GE *__restrict__ maskedX,
+                      const uint8_t *__restrict__ key, const uint8_t *__restrict__ seed, uint32_t party,
+                      const GE *__restrict__ left, const GE *__restrict__ right, const GE *__restrict__ lut,
+                      uint32_t lutNum, uint32_t m, uint32_t n, size_t N, uint32_t G, uint32_t j0)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const size_t   work  = ((N * G + 31) / 32) * 32; // whole warps stay in the loop (shuffles)
+    const uint32_t lg    = threadIdx.x % G;
+    const uint32_t jcnt  = lutNum > j0 ? min((uint32_t)LMAX, lutNum - j0) : 0u;
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t i      = w / G;
+        const bool   active = i < N;
+        uint64_t     E = 0, T[LMAX];
+#pragma unroll
+        for (int k = 0; k < LMAX; k++) T[k] = 0;
+        if (active)
+        {
+            GrottoKeyView<GE> K;
+            K.set(key, n, i, N);
+            const uint64_t mx = (uint64_t)__ldg(maskedX + i);
+            for (uint32_t q = lg; q < m; q += G)
+            {
+                const uint64_t bit = grotto_interval_bit<GE>(A, K, seed + 16 * i, party, n, mx,
+                                                             (uint64_t)__ldg(left + q), (uint64_t)__ldg(right + q));
+                E += bit;
+#pragma unroll
+                for (int k = 0; k < LMAX; k++)
+                    if ((uint32_t)k < jcnt) T[k] += bit * (uint64_t)__ldg(lut + q + (size_t)(j0 + k) * m);
+            }
+        }
+        for (uint32_t off = G >> 1; off > 0; off >>= 1)
+        {
+            E += __shfl_xor_sync(0xffffffffu, E, off);
+#pragma unroll
+            for (int k = 0; k < LMAX; k++) T[k] += __shfl_xor_sync(0xffffffffu, T[k], off);
+        }
+        if (active && lg == 0)
+        {
+            if (party)
+            {
+                E = 0 - E;
+#pragma unroll
+                for (int k = 0; k < LMAX; k++) T[k] = 0 - T[k];
+            }
+            if (j0 == 0) outE[i] = (GE)E;
+#pragma unroll
+            for (int k = 0; k < LMAX; k++)
+                if ((uint32_t)k < jcnt) outT[i * lutNum + j0 + k] = (GE)T[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Full domain. One thread expands a subtree of depth d (2^d leaves) below a node reached by
+// walking the top D - d levels, expanding both children of every internal node once
+// (key schedule + 2 blocks) and keeping right siblings on a small stack. Each leaf j yields
+// the 64-bit word u_j (equality shares of x = 64 j .. 64 j + 63) and the right-turn parity
+// P_j; the comparison row is excl_prefix_xor(u_j) ^ (P_j ^ party ? ~0 : 0).
+// ---------------------------------------------------------------------------------------
+constexpr int kAllMaxSub = 5;
+
+__device__ __forceinline__ uint64_t excl_prefix_xor(uint64_t u)
+{
+    uint64_t p = u;
+    p ^= p << 1;
+    p ^= p << 2;
+    p ^= p << 4;
+    p ^= p << 8;
+    p ^= p << 16;
+    p ^= p << 32;
+    return p << 1;
+}
+
+template <typename GE, int MODE> // MODE 0: equality rows, 1: comparison (equalBound) rows
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_all_kernel(unsigned long long *__restrict__ out, const uint8_t *__restrict__ key,
+                      const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, size_t N, uint32_t d)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const uint32_t D     = n - 6;
+    const uint32_t top   = D - d;
+    const size_t   S     = (size_t)1 << top;
+    const size_t   work  = N * S;
+    const size_t   words = (size_t)1 << D; // leaf words per key
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t      i = w / S, sub = w % S;
+        GrottoKeyView<GE> K;
+        K.set(key, n, i, N);
+        uint32_t s[4];
+        load_block_be(seed + 16 * i, s);
+        s[0] &= ~kSeedTBit;
+        uint32_t t = party, par = 0;
+        for (uint32_t lv = 0; lv < top; lv++)
+        {
+            const uint32_t dir = (uint32_t)((sub >> (top - 1 - lv)) & 1u);
+            const uint32_t tn  = grotto_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv);
+            par ^= dir & (t ^ tn);
+            t = tn;
+        }
+        // right-sibling stack: seed words, control bit, parity per depth below the subtree root
+        uint32_t           stk[kAllMaxSub][6];
+        uint32_t           depth = 0;
+        const size_t       nleaf = (size_t)1 << d;
+        unsigned long long *row  = out + i * words + sub * nleaf;
+        for (size_t j = 0; j < nleaf; j++)
+        {
+            while (depth < d)
+            {
+                const uint32_t lv = top + depth;
+                uint32_t       cw[4];
+                load_block_be(K.sCW + 16 * lv, cw);
+                uint32_t st[2][4];
+                prg_block(st[0], 0);
+                prg_block(st[1], 1);
+                aes_encrypt<2>(A, s, st);
+                const uint32_t m  = 0u - t;
+                uint32_t       tL = (st[0][0] >> 24) & 1u, tR = (st[1][0] >> 24) & 1u;
+                st[0][0] &= ~kSeedTBit;
+                st[1][0] &= ~kSeedTBit;
+                tL ^= (uint32_t)((K.tl >> lv) & 1u) & t;
+                tR ^= (uint32_t)((K.tr >> lv) & 1u) & t;
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+                {
+                    stk[depth][c] = st[1][c] ^ (cw[c] & m);
+                    s[c]          = st[0][c] ^ (cw[c] & m);
+                }
+                stk[depth][4] = tR;
+                stk[depth][5] = par ^ (t ^ tR);
+                t             = tL;
+                depth++;
+            }
+            const uint64_t u0 = hi_u64(s);
+            const uint64_t u  = t ? (u0 ^ K.last) : u0;
+            if (MODE == 0)
+                row[j] = u;
+            else
+                row[j] = excl_prefix_xor(u) ^ ((par ^ party) ? ~0ull : 0ull);
+            if (j + 1 < nleaf)
+            {
+                // next leaf: right sibling at depth d - 1 - ctz(j + 1)
+                const uint32_t p = (uint32_t)__ffsll((long long)(j + 1)) - 1;
+                depth            = d - 1 - p;
+#pragma unroll
+                for (int c = 0; c < 4; c++) s[c] = stk[depth][c];
+                t   = stk[depth][4];
+                par = stk[depth][5];
+                depth++;
+            }
+        }
+    }
+}
+
+static inline size_t grotto_key_bytes(size_t n, size_t es, size_t N)
+{
+    return N * (16 * (n - 6) + 8 + 2 * es);
+}
+
+static inline size_t grotto_cache_bytes(size_t n, size_t N)
+{
+    return N * (16 * (n - 6) + (n - 6));
+}
+
+template <typename K, typename... Args>
+static int launch(K kern, size_t work, cudaStream_t stream, Args... args)
+{
+    if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
+    kern<<<grid_for(work, kGrottoThreads, 1), kGrottoThreads, kAesSmemTotal, stream>>>(args...);
+    return launch_status();
+}
+
+} // namespace fss
+
+using namespace fss;
+
+// Validation order: GrottoKeyGenTask::check (src/kernel/grotto.h:26-47).
+extern "C" FAST_FSS_API int FastFss_cuda_grottoKeyGen(void *key, size_t keyDataSize, const void *alpha,
+                                                      size_t alphaDataSize, const void *seed0, size_t seedDataSize0,
+                                                      const void *seed1, size_t seedDataSize1, size_t bitWidthIn,
+                                                      size_t elementSize, size_t elementNum, void *cudaStreamPtr)
+{
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum;
+        if (!(6 <= bitWidthIn && bitWidthIn <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (alphaDataSize != N * es) return FAST_FSS_INVALID_ALPHA_DATA_SIZE_ERROR;
+        if (seedDataSize0 != N * 16 || seedDataSize1 != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (keyDataSize != grotto_key_bytes(bitWidthIn, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (N == 0) return FAST_FSS_SUCCESS;
+        return launch(grotto_keygen_kernel<GE>, N, resolve_stream(cudaStreamPtr), (uint8_t *)key, (const GE *)alpha,
+                      (const uint8_t *)seed0, (const uint8_t *)seed1, (uint32_t)bitWidthIn, N);
+    });
+}
+
+// Shared checks of GrottoEqEvalTask / GrottoEvalTask (src/kernel/grotto.h:77-114,155-192).
+template <typename GE>
+static int grotto_point_checks(size_t sharedOutDataSize, size_t maskedXDataSize, size_t keyDataSize,
+                               size_t seedDataSize, int partyId, size_t n, size_t N, size_t cacheDataSize)
+{
+    const size_t es = sizeof(GE);
+    if (!(6 <= n && n <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+    if (sharedOutDataSize != N * es) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+    if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+    if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+    if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+    if (keyDataSize != grotto_key_bytes(n, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+    if (cacheDataSize != 0 && cacheDataSize != grotto_cache_bytes(n, N)) return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+    return FAST_FSS_SUCCESS;
+}
+
+extern "C" FAST_FSS_API int FastFss_cuda_grottoEqEval(void *sharedBooleanOut, size_t sharedOutDataSize,
+                                                      const void *maskedX, size_t maskedXDataSize, const void *key,
+                                                      size_t keyDataSize, const void *seed, size_t seedDataSize,
+                                                      int partyId, size_t bitWidthIn, size_t elementSize,
+                                                      size_t elementNum, void *cache, size_t cacheDataSize,
+                                                      void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE = decltype(tag);
+        int rc   = grotto_point_checks<GE>(sharedOutDataSize, maskedXDataSize, keyDataSize, seedDataSize, partyId,
+                                         bitWidthIn, elementNum, cacheDataSize);
+        if (rc != FAST_FSS_SUCCESS || elementNum == 0) return rc;
+        return launch(grotto_eval_kernel<GE, 0>, elementNum, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
+                      (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                      (uint32_t)bitWidthIn, false, elementNum);
+    });
+}
+
+extern "C" FAST_FSS_API int FastFss_cuda_grottoEval(void *sharedBooleanOut, size_t sharedOutDataSize,
+                                                    const void *maskedX, size_t maskedXDataSize, const void *key,
+                                                    size_t keyDataSize, const void *seed, size_t seedDataSize,
+                                                    bool equalBound, int partyId, size_t bitWidthIn,
+                                                    size_t elementSize, size_t elementNum, void *cache,
+                                                    size_t cacheDataSize, void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE = decltype(tag);
+        int rc   = grotto_point_checks<GE>(sharedOutDataSize, maskedXDataSize, keyDataSize, seedDataSize, partyId,
+                                         bitWidthIn, elementNum, cacheDataSize);
+        if (rc != FAST_FSS_SUCCESS || elementNum == 0) return rc;
+        return launch(grotto_eval_kernel<GE, 1>, elementNum, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
+                      (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                      (uint32_t)bitWidthIn, equalBound, elementNum);
+    });
+}
+
+// Validation order: GrottoMICEvalTask::check (src/kernel/grotto.h:236-278).
+extern "C" FAST_FSS_API int FastFss_cuda_grottoMICEval(void *sharedBooleanOut, size_t sharedBooleanOutDataSize,
+                                                       const void *maskedX, size_t maskedXDataSize, const void *key,
+                                                       size_t keyDataSize, const void *seed, size_t seedDataSize,
+                                                       int partyId, const void *leftEndpoints,
+                                                       size_t leftEndpointsDataSize, const void *rightEndpoints,
+                                                       size_t rightEndpointsDataSize, size_t bitWidthIn,
+                                                       size_t elementSize, size_t elementNum, void *cache,
+                                                       size_t cacheDataSize, void *cudaStreamPtr)
+{
+    (void)cache;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum, n = bitWidthIn;
+        if (!(6 <= n && n <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        const size_t m = leftEndpointsDataSize / es;
+        if (m * es != leftEndpointsDataSize || m * es != rightEndpointsDataSize)
+            return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
+        if (sharedBooleanOutDataSize != N * es * m) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (keyDataSize != grotto_key_bytes(n, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (cacheDataSize != 0 && cacheDataSize != grotto_cache_bytes(n, N))
+            return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+        if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
+        return launch(grotto_mic_kernel<GE>, N * m, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
+                      (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                      (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)n, N);
+    });
+}
+
+// Validation order: GrottoIntervalLutEvalTask::check (src/kernel/grotto.h:330-381). With no
+// intervals the reference's modulo by (elementSize * intervalNum) is undefined; this
+// library reports an invalid lookup table instead.
+extern "C" FAST_FSS_API int FastFss_cuda_grottoIntervalLutEval(
+    void *sharedOutE, size_t sharedOutEDataSize, void *sharedOutT, size_t sharedOutTDataSize, const void *maskedX,
+    size_t maskedXDataSize, const void *key, size_t keyDataSize, const void *seed, size_t seedDataSize, int partyId,
+    const void *leftEndpoints, size_t leftEndpointsDataSize, const void *rightEndpoints, size_t rightEndpointsDataSize,
+    const void *lookUpTable, size_t lookUpTableDataSize, size_t bitWidthIn, size_t bitWidthOut, size_t elementSize,
+    size_t elementNum, void *cache, size_t cacheDataSize, void *cudaStreamPtr)
+{
+    (void)cache, (void)bitWidthOut;
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum, n = bitWidthIn;
+        if (!(6 <= n && n <= es * 8)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(leftEndpointsDataSize == rightEndpointsDataSize && leftEndpointsDataSize % es == 0))
+            return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
+        const size_t m = leftEndpointsDataSize / es;
+        if (m == 0 || lookUpTableDataSize % (es * m) != 0) return FAST_FSS_INVALID_LOOKUP_TABLE_DATA_SIZE_ERROR;
+        const size_t lutNum = lookUpTableDataSize / (es * m);
+        if (sharedOutEDataSize != N * es) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (sharedOutTDataSize != N * es * lutNum) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (keyDataSize != grotto_key_bytes(n, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (cacheDataSize != 0 && cacheDataSize != grotto_cache_bytes(n, N))
+            return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
+        if (N == 0) return FAST_FSS_SUCCESS;
+        uint32_t G = 1;
+        while (G < 32 && G < m) G <<= 1;
+        cudaStream_t stream = resolve_stream(cudaStreamPtr);
+        constexpr int LMAX = 4;
+        for (size_t j0 = 0; j0 < (lutNum ? lutNum : 1); j0 += LMAX)
+        {
+            const int rc = launch(grotto_lut_kernel<GE, LMAX>, N * G, stream, (GE *)sharedOutE, (GE *)sharedOutT,
+                                  (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                                  (const GE *)leftEndpoints, (const GE *)rightEndpoints, (const GE *)lookUpTable,
+                                  (uint32_t)lutNum, (uint32_t)m, (uint32_t)n, N, G, (uint32_t)j0);
+            if (rc != FAST_FSS_SUCCESS) return rc;
+        }
+        return FAST_FSS_SUCCESS;
+    });
+}
+
+template <int MODE>
+static int grotto_all_entry(void *out, size_t outDataSize, const void *key, size_t keyDataSize, const void *seed,
+                            size_t seedDataSize, int partyId, size_t bitWidthIn, size_t elementSize,
+                            size_t elementNum, void *cudaStreamPtr)
+{
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum, n = bitWidthIn;
+        if (!(6 <= n && n <= es * 8 && n <= FAST_FSS_GROTTO_ALL_MAX_BITWIDTH)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (keyDataSize != grotto_key_bytes(n, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (seedDataSize != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
+        if (outDataSize != N * (((size_t)1 << n) / 8)) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (((uintptr_t)out & 7u) != 0) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (N == 0) return FAST_FSS_SUCCESS;
+        const uint32_t D = (uint32_t)n - 6;
+        const uint32_t d = D < (uint32_t)kAllMaxSub ? D : (uint32_t)kAllMaxSub;
+        return launch(grotto_all_kernel<GE, MODE>, N << (D - d), resolve_stream(cudaStreamPtr),
+                      (unsigned long long *)out, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                      (uint32_t)n, N, d);
+    });
+}
+
+extern "C" FAST_FSS_API int FastFss_cuda_grottoEqEvalAll(void *outBits, size_t outBitsDataSize, const void *key,
+                                                         size_t keyDataSize, const void *seed, size_t seedDataSize,
+                                                         int partyId, size_t bitWidthIn, size_t elementSize,
+                                                         size_t elementNum, void *cudaStreamPtr)
+{
+    return grotto_all_entry<0>(outBits, outBitsDataSize, key, keyDataSize, seed, seedDataSize, partyId, bitWidthIn,
+                               elementSize, elementNum, cudaStreamPtr);
+}
+
+extern "C" FAST_FSS_API int FastFss_cuda_grottoLeEvalAll(void *outBits, size_t outBitsDataSize, const void *key,
+                                                         size_t keyDataSize, const void *seed, size_t seedDataSize,
+                                                         int partyId, size_t bitWidthIn, size_t elementSize,
+                                                         size_t elementNum, void *cudaStreamPtr)
+{
+    return grotto_all_entry<1>(outBits, outBitsDataSize, key, keyDataSize, seed, seedDataSize, partyId, bitWidthIn,
+                               elementSize, elementNum, cudaStreamPtr);
+}

@@ -3,8 +3,8 @@
  * FastFss_b200_smemLookupProbe measures the sustained rate of conflict-free, byte-permute
  * addressed 32-bit shared-memory table lookups — the access the AES T-table rounds of every
  * FSS kernel are built from — so a benchmark can report kernel throughput as a fraction of
- * a measured peak. It launches one 512-thread CTA per SM; each thread runs 8 independent
- * lookup chains for `iterations` steps and stores one word per thread into `sink`
+ * a measured peak. It launches one 512-thread CTA per SM; each thread issues 16 independent
+ * lookups per iteration for `iterations` iterations and stores one word per thread into `sink`
  * (sinkBytes >= 4 * 512 * SM count). *lookups receives the total number of lookups issued.
  * Asynchronous on *(cudaStream_t *)cudaStreamPtr (cudaStreamPerThread when NULL). */
 #ifndef FAST_FSS_B200_DIAG_H
