@@ -50,7 +50,7 @@ ALGO_BYTES_PER_ELEM = KEY_BYTES_PER_ELEM + 16 + ES + ES  # key + seed + maskedX 
 LOOKUPS_PER_ELEM = N_BITS * (40 + 160 + 134)
 AES_BLOCKS_PER_ELEM = 2 * N_BITS
 AES_KS_PER_ELEM = N_BITS
-METRIC = "DCF eval Gelem/s at n=32 (Z_2^32)"
+METRIC = "DCF eval Gelem/s at n=32 (Z_2^32), plain vs batched; serving p50/p99 ms"
 UNIT = "Gelem/s"
 CONFIG = {"workload": "plain DCF eval, 2^24 elements, n=32, Z_2^32 (uint32), groupSize 1, one party per step",
           "elements_per_rank": N_ELEMENTS, "bitWidthIn": N_BITS, "bitWidthOut": N_BITS, "elementSize": ES,
@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--elements", type=int, default=N_ELEMENTS)
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="wall budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
+    ap.add_argument("--batched-instances", type=int, default=256)
+    ap.add_argument("--serving-requests", type=int, default=160)
     return ap.parse_args()
 
 
@@ -404,11 +407,88 @@ def main():
         "clocks": ck,
         "shares_reconstruct": ok,
     }
+    if not args.no_extras:
+        line["batched"] = batched_section(dev, args)
+        line["serving"] = serving_section(dev, args)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_rate(args.cpu_seconds)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def batched_section(dev, args) -> dict:
+    """Mixed-bitwidth MIC + spline batch: plain per-call C-ABI loop vs one persistent launch
+    (autotuned, CUDA-graph captured), same instances, same stream; elements/s of both."""
+    import torch
+
+    from fastfunctionsecretsharing_b200 import batch as B
+    from fastfunctionsecretsharing_b200 import workloads as W
+
+    mic_log2, spline_log2 = (8, 18), (8, 13)
+    inst = W.mixed_mic_spline(device=dev, instances=args.batched_instances, seed=4, mic_log2=mic_log2,
+                              spline_log2=spline_log2)
+    elems = sum(i.N for i in inst)
+    stream = torch.cuda.current_stream(dev)
+    steps = max(3, min(args.steps, 10))
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    plain_ms = timed(lambda: W.run_plain(inst))
+    b = B.Batch([i.request for i in inst], dev)
+    best, timings = B.autotune(b, reps=2)
+    g = b.graph()
+    batched_ms = timed(g.replay)
+    same = all(torch.equal(i.request.tensors[0].view(-1), i.out_plain.view(-1)) for i in inst)
+    res = {"workload": (f"{args.batched_instances} instances: half DCF-MIC (16 sorted intervals, n in "
+                        "{8,12,16,24,32,64}, N log-uniform 2^8..2^18), half spline (32 intervals, degree 2, "
+                        "n=bo=64, N log-uniform 2^8..2^13); one party; keys device-resident"),
+           "elements_per_step": elems, "plain_ms": plain_ms, "batched_ms": batched_ms,
+           "plain_elem_per_s": elems / (plain_ms / 1e3), "batched_elem_per_s": elems / (batched_ms / 1e3),
+           "speedup": plain_ms / batched_ms, "plain_launches_per_step": len(inst),
+           "batched_launches_per_step": 1, "tuning": list(best.as_tuple()),
+           "autotune_ms": {str(k): v for k, v in timings.items()}, "outputs_match_plain": bool(same),
+           "estimated_lookups": b.plan.lookups}
+    del inst, b, g
+    torch.cuda.empty_cache()
+    return res
+
+
+def serving_section(dev, args) -> dict:
+    """Continuous-batching server vs plain per-call serving on the same Poisson arrivals."""
+    import torch
+
+    from fastfunctionsecretsharing_b200 import serving as S
+
+    P = S.make_pools(dev, dcf_log2=(10, 20), spline_log2=(10, 14))
+    out = {"workload": ("12-layer MLP (width 4096, batch 64) trace: 2^18 ReLU DCFs (n=32) + 2^18 GeLU splines "
+                        "(n=64, 32 intervals, degree 2) per layer, issued as requests of 2^k elements (DCF k in "
+                        "10..20, spline k in 10..14); key store 64 GB charged per request; 4 stream slots"),
+           "rates": []}
+    for rate in (100.0, 1000.0, 10000.0):
+        row = {"rate_req_per_s": rate}
+        for mode in ("batched", "plain"):
+            reqs = S.make_requests(P, rate=rate, count=args.serving_requests, seed=int(rate))
+            srv = S.Server(P, capacity_bytes=64 << 30, slots=4)
+            makespan = srv.run(reqs, mode=mode)
+            st = S.summarize(reqs, makespan)
+            st["launches"] = srv.launches
+            st["key_store_peak_gb"] = srv.store.peak / 2**30
+            row[mode] = st
+        out["rates"].append(row)
+    del P
+    torch.cuda.empty_cache()
+    return out
 
 
 def seed1_regen(gen_seed: int, N: int, dev):

@@ -12,6 +12,7 @@
 #include <FastFss/cuda/dpf.h>
 #include <FastFss/dpf.h>
 
+#include "dpf_core.cuh"
 #include "fss_device.cuh"
 #include "fss_host.h"
 
@@ -86,42 +87,6 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
             if (t1) v = 0 - v;
             kb[2 + j] = (GE)v;
         }
-    }
-}
-
-// Walks one element's tree along x (already reduced mod 2^n) and writes the g outputs.
-template <typename GE>
-__device__ __forceinline__ void dpf_eval_point(const AesLanes &A, GE *o, const uint8_t *sCWp, const GE *kb,
-                                               const uint8_t *seed, uint32_t party, uint32_t n, uint32_t bo,
-                                               uint32_t g, uint64_t x, uint64_t tl, uint64_t tr)
-{
-    uint32_t s[4];
-    load_block_be(seed, s);
-    s[0] &= ~kSeedTBit;
-    uint32_t t = party;
-#pragma unroll 1
-    for (uint32_t lv = 0; lv < n; lv++)
-    {
-        uint32_t cw[4];
-        load_block_be(sCWp + 16 * lv, cw);
-        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
-        uint32_t       st[1][4];
-        prg_block(st[0], dir);
-        aes_encrypt<1>(A, s, st);
-        uint32_t       tn = (st[0][0] >> 24) & 1u;
-        const uint32_t m  = 0u - t;
-        st[0][0] &= ~kSeedTBit;
-#pragma unroll
-        for (int c = 0; c < 4; c++) s[c] = st[0][c] ^ (cw[c] & m);
-        tn ^= (uint32_t)(((dir ? tr : tl) >> lv) & 1u) & t;
-        t = tn;
-    }
-    ConvertStream cv;
-    cv.init(s, bo, g);
-    for (uint32_t j = 0; j < g; j++)
-    {
-        const uint64_t v = cv.value(A, j) + (t ? (uint64_t)__ldg(kb + 2 + j) : 0);
-        o[j]             = (GE)(party ? (0 - v) : v);
     }
 }
 

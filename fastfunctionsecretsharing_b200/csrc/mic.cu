@@ -14,6 +14,7 @@
 #include "dcf_core.cuh"
 #include "fss_device.cuh"
 #include "fss_host.h"
+#include "mic_core.cuh"
 
 namespace fss {
 
@@ -62,22 +63,7 @@ __global__ void __launch_bounds__(kMicThreads, 1)
     const size_t work = N * m;
     A.init();
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
-    {
-        const size_t   i = w / m, q = w % m;
-        DcfKeyView<GE> K;
-        K.set(key, n, 1, i, N);
-        const uint64_t x  = mod_bits<GE>((uint64_t)__ldg(maskedX + i), n);
-        const uint64_t L  = (uint64_t)__ldg(left + q), R = (uint64_t)__ldg(right + q);
-        const uint64_t qP = mod_bits<GE>((uint64_t)(GE)(R + 1), n);
-        const uint64_t xP = mod_bits<GE>((uint64_t)(GE)(x - 1 - L), n);
-        const uint64_t xQ = mod_bits<GE>((uint64_t)(GE)(x - 1 - qP), n);
-        const uint64_t p  = mod_bits<GE>(L, n);
-        const uint64_t sp = dcf_eval_g1<GE>(A, K, seed + 16 * i, party, n, bo, xP);
-        const uint64_t sq = dcf_eval_g1<GE>(A, K, seed + 16 * i, party, n, bo, xQ);
-        uint64_t       o  = sq - sp + (uint64_t)__ldg(z + w);
-        if (party == 1) o += (uint64_t)((int64_t)(x > p) - (int64_t)(x > qP));
-        out[w] = (GE)o;
-    }
+        out[w] = mic_eval_item<GE>(A, maskedX, key, z, seed, party, left, right, m, n, bo, N, w);
 }
 
 static inline size_t dcf_key_bytes_g1(size_t n, size_t es, size_t N)

@@ -19,11 +19,11 @@
 #include "dcf_core.cuh"
 #include "fss_device.cuh"
 #include "fss_host.h"
+#include "spline_core.cuh"
 
 namespace fss {
 
 constexpr int kSplineThreads = 256;
-constexpr int kSplineMaxC    = 4; // coefficients reduced per pass
 
 // splineShiftPolynomialCoefficients (src/impl/spline.h:89-117), writing d + 1 values.
 template <typename GE>
@@ -86,72 +86,10 @@ __global__ void __launch_bounds__(kSplineThreads, 1)
     aes_tables_build();
     AesLanes A;
     A.init();
-    const uint32_t cn = d + 1, g = m * cn;
-    const size_t   work = ((N * G + 31) / 32) * 32; // whole warps stay in the loop (shuffles)
-    const uint32_t lg   = threadIdx.x % G;
+    const size_t work = ((N * G + 31) / 32) * 32; // whole warps stay in the loop (shuffles)
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
-    {
-        const size_t   i      = w / G;
-        const bool     active = i < N;
-        DcfKeyView<GE> K;
-        uint64_t       x = 0;
-        if (active)
-        {
-            K.set(key, n, g, i, N);
-            x = mod_bits<GE>((uint64_t)__ldg(maskedX + i), n);
-        }
-        uint64_t result = 0, xpow = 1;
-        for (uint32_t c0 = 0; c0 < cn; c0 += kSplineMaxC)
-        {
-            const uint32_t cnt = min((uint32_t)kSplineMaxC, cn - c0);
-            uint64_t       acc[kSplineMaxC];
-#pragma unroll
-            for (int k = 0; k < kSplineMaxC; k++) acc[k] = 0;
-            if (active)
-            {
-                for (uint32_t q = lg; q < m; q += G)
-                {
-                    const uint64_t L  = mod_bits<GE>((uint64_t)__ldg(left + q), n);
-                    const uint64_t R  = mod_bits<GE>((uint64_t)__ldg(right + q), n);
-                    const uint64_t Rp = mod_bits<GE>((uint64_t)(GE)(R + 1), n);
-                    uint64_t       sL[kSplineMaxC], sR[kSplineMaxC];
-#pragma unroll
-                    for (int k = 0; k < kSplineMaxC; k++) sL[k] = 0, sR[k] = 0;
-                    dcf_eval_slice<GE, kSplineMaxC>(A, sL, K, seed + 16 * i, party, n, bo, g,
-                                                    mod_bits<GE>((uint64_t)(GE)(x - 1 - L), n), q * cn + c0, cnt);
-                    dcf_eval_slice<GE, kSplineMaxC>(A, sR, K, seed + 16 * i, party, n, bo, g,
-                                                    mod_bits<GE>((uint64_t)(GE)(x - 1 - Rp), n), q * cn + c0, cnt);
-                    const uint64_t cx = (uint64_t)((int64_t)(x > L) - (int64_t)(x > Rp));
-#pragma unroll
-                    for (int k = 0; k < kSplineMaxC; k++)
-                    {
-                        if ((uint32_t)k < cnt)
-                        {
-                            const size_t   o = i * g + q * cn + c0 + k;
-                            const uint64_t b = (uint64_t)__ldg(sharedBeta + o);
-                            acc[k] += cx * b - sL[k] + sR[k] + (uint64_t)__ldg(sharedE + o);
-                        }
-                    }
-                }
-            }
-            for (uint32_t off = G >> 1; off > 0; off >>= 1)
-            {
-#pragma unroll
-                for (int k = 0; k < kSplineMaxC; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
-            }
-            // splineEvaluatePolynomial (src/impl/spline.h:119-135): sum of acc_c x^c
-#pragma unroll
-            for (int k = 0; k < kSplineMaxC; k++)
-            {
-                if ((uint32_t)k < cnt)
-                {
-                    result += acc[k] * xpow;
-                    xpow *= x;
-                }
-            }
-        }
-        if (active && lg == 0) out[i] = (GE)mod_bits<GE>((uint64_t)(GE)result, bo);
-    }
+        spline_eval_group<GE>(A, out, maskedX, key, sharedE, sharedBeta, seed, party, left, right, m, d, n, bo, N, G,
+                              w / G, (uint32_t)(w % G), w / G < N);
 }
 
 static inline size_t dcf_key_bytes(size_t n, size_t g, size_t es, size_t N)

@@ -1,0 +1,317 @@
+"""Continuous-batching FSS evaluation server, driven by a simulated two-party inference engine.
+
+The engine runs a 12-layer MLP (width 4096, batch 64); every layer needs 2^18 ReLU
+comparisons (DCF, n = 32 over Z_2^32) and 2^18 GeLU splines (32 intervals, degree 2,
+n = 64 over Z_2^64). It issues that work as requests of 2^k elements (k uniform), arriving
+as a Poisson process. The server
+
+* keeps key material device-resident in a key store whose capacity is counted in bytes; a
+  request is admitted only when its keys fit in the remaining capacity (charged on
+  admission, released on completion);
+* batches continuously: whatever has been admitted since the last launch goes out as one
+  persistent batched launch on a free stream slot while earlier batches are still running on
+  the other slots (up to `slots` launches in flight); a request's masked input is copied in
+  from pinned host memory and its shares copied back on the same stream;
+* records per-request latency (completion - arrival, wall clock; completion is observed by
+  polling the launch's CUDA event).
+
+The `plain` mode serves the same arrivals without batching: every admitted request is its own
+per-call C-ABI evaluation, queued FIFO on one stream.
+
+Key material: the store charges every request its key bytes; the kernels read valid keys from
+one pool per kind and size class, so every evaluation is real and checkable while the 64 GB
+model stays within one GPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib, batch
+from . import dcf_key_gen, spline_get_cache_data_size, spline_key_gen
+from .workloads import _rand_ring, _ring_tensor, partition
+
+DCF_N = 32
+SPLINE_N, SPLINE_M, SPLINE_D = 64, 32, 2
+SPLINE_G = SPLINE_M * (SPLINE_D + 1)
+DCF_KEY_BYTES = 16 * DCF_N + 4 * DCF_N + 3 * 4  # per element (652)
+SPLINE_KEY_BYTES = 16 * SPLINE_N + 8 * SPLINE_N * SPLINE_G + 2 * 8 + 8 * SPLINE_G  # per element (50,960)
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str  # "dcf" or "spline"
+    layer: int
+    size: int
+    arrival: float
+    key_bytes: int
+    start: float = 0.0
+    done: float = 0.0
+    x_host: torch.Tensor | None = None
+    out_host: torch.Tensor | None = None
+
+
+@dataclass
+class SizeClass:
+    """Valid keys (and the other per-element key material) for requests of N elements."""
+
+    N: int
+    key: torch.Tensor
+    seed: torch.Tensor
+    e: torch.Tensor | None = None
+    beta: torch.Tensor | None = None
+
+
+@dataclass
+class Pools:
+    dev: torch.device
+    party: int
+    dcf: dict = field(default_factory=dict)
+    spline: dict = field(default_factory=dict)
+    spline_L: torch.Tensor | None = None
+    spline_R: torch.Tensor | None = None
+
+
+def make_pools(device, dcf_log2=(10, 20), spline_log2=(10, 14), seed=9, party=0) -> Pools:
+    """Generates (on the device) keys for every power-of-two request size."""
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    P = Pools(dev, party)
+    for k in range(dcf_log2[0], dcf_log2[1] + 1):
+        N = 1 << k
+        a, b = _rand_ring(gen, (N,), 4, dev), _rand_ring(gen, (N,), 4, dev)
+        s0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+        s1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+        key = torch.empty(0, dtype=torch.uint8, device=dev)
+        dcf_key_gen(key, a, b, s0, s1, DCF_N, DCF_N, 1)
+        P.dcf[N] = SizeClass(N, key, s0 if party == 0 else s1)
+    L, R = partition(rng, SPLINE_M, SPLINE_N)
+    P.spline_L, P.spline_R = _ring_tensor(L, 8, dev), _ring_tensor(R, 8, dev)
+    coeffs = [int(round(rng.uniform(-4, 4) * 65536)) for _ in range(SPLINE_G)]
+    ct = _ring_tensor(coeffs, 8, dev)
+    for k in range(spline_log2[0], spline_log2[1] + 1):
+        N = 1 << k
+        a = _rand_ring(gen, (N,), 8, dev)
+        s0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+        s1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+        key = torch.empty(0, dtype=torch.uint8, device=dev)
+        e = torch.empty(0, dtype=torch.int64, device=dev)
+        beta = torch.empty(0, dtype=torch.int64, device=dev)
+        spline_key_gen(key, e, beta, a, s0, s1, ct, SPLINE_D, P.spline_L, P.spline_R, SPLINE_M, SPLINE_N, SPLINE_N)
+        e0, b0 = _rand_ring(gen, e.shape, 8, dev), _rand_ring(gen, beta.shape, 8, dev)
+        if party == 1:
+            e0, b0 = e - e0, beta - b0
+        P.spline[N] = SizeClass(N, key, s0 if party == 0 else s1, e0, b0)
+    torch.cuda.synchronize(dev)
+    return P
+
+
+class KeyStore:
+    """Device-resident key budget; a request's keys are charged on admission."""
+
+    def __init__(self, capacity_bytes: int):
+        self.capacity = capacity_bytes
+        self.used = 0
+        self.peak = 0
+
+    def try_admit(self, nbytes: int) -> bool:
+        if self.used + nbytes > self.capacity:
+            return False
+        self.used += nbytes
+        self.peak = max(self.peak, self.used)
+        return True
+
+    def release(self, nbytes: int) -> None:
+        self.used -= nbytes
+
+
+def mlp_trace(rng: np.random.Generator, layers=12, width=4096, batch_rows=64, lo=10, hi=20, spline_hi=14,
+              limit: int | None = None):
+    """Splits every layer's width * batch_rows DCF and spline evaluations into requests of 2^k
+    elements, k uniform in [lo, hi] (spline: [lo, spline_hi]), alternating the two kinds."""
+    per_layer = width * batch_rows
+    reqs = []
+    for layer in range(layers):
+        left = {"dcf": per_layer, "spline": per_layer}
+        while left["dcf"] > 0 or left["spline"] > 0:
+            for kind, top in (("dcf", hi), ("spline", min(hi, spline_hi))):
+                if left[kind] <= 0:
+                    continue
+                size = 1 << int(rng.integers(lo, top + 1))
+                while size > left[kind]:
+                    size >>= 1
+                reqs.append((kind, layer, size))
+                left[kind] -= size
+                if limit and len(reqs) >= limit:
+                    return reqs
+    return reqs
+
+
+def make_requests(P: Pools, rate: float, count: int, seed: int = 1, dcf_log2=(10, 20), spline_log2=(10, 14)):
+    """`count` requests of the MLP trace with Poisson arrivals at `rate` per second (arrival
+    times relative to the start). Host inputs and outputs are pinned."""
+    rng = np.random.default_rng(seed)
+    trace = mlp_trace(rng, lo=dcf_log2[0], hi=dcf_log2[1], spline_hi=spline_log2[1], limit=count)
+    t = 0.0
+    out = []
+    for rid, (kind, layer, size) in enumerate(trace[:count]):
+        t += rng.exponential(1.0 / rate)
+        if kind == "dcf":
+            xb = torch.from_numpy(rng.integers(-2**31, 2**31, size=size, dtype=np.int64).astype(np.int32)).pin_memory()
+            ob = torch.empty(size, dtype=torch.int32).pin_memory()
+            kb = size * DCF_KEY_BYTES
+        else:
+            xb = torch.from_numpy(rng.integers(-2**63, 2**63 - 1, size=size, dtype=np.int64)).pin_memory()
+            ob = torch.empty(size, dtype=torch.int64).pin_memory()
+            kb = size * SPLINE_KEY_BYTES
+        out.append(Request(rid, kind, layer, size, t, kb, x_host=xb, out_host=ob))
+    return out
+
+
+class Server:
+    def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=4, tuning: batch.Tuning | None = None):
+        self.P = pools
+        self.dev = pools.dev
+        self.store = KeyStore(capacity_bytes)
+        self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
+        self.tuning = tuning or batch.Tuning(256, 1 << 21, 0, 0)
+        self.launches = 0
+
+    def _build(self, r: Request) -> batch.Request:
+        """Device buffers and the batch request of r (input copied in on the current stream)."""
+        P = self.P
+        if r.kind == "dcf":
+            c = P.dcf[r.size]
+            x = torch.empty(r.size, dtype=torch.int32, device=self.dev)
+            x.copy_(r.x_host, non_blocking=True)
+            out = torch.empty(0, dtype=torch.int32, device=self.dev)
+            return batch.dcf_request(out, x, c.key, c.seed, P.party, DCF_N, DCF_N)
+        c = P.spline[r.size]
+        x = torch.empty(r.size, dtype=torch.int64, device=self.dev)
+        x.copy_(r.x_host, non_blocking=True)
+        out = torch.empty(0, dtype=torch.int64, device=self.dev)
+        return batch.spline_request(out, x, c.key, c.e, c.beta, c.seed, P.party, P.spline_L, P.spline_R, SPLINE_M,
+                                    SPLINE_D, SPLINE_N, SPLINE_N)
+
+    def _plain_call(self, r: Request, stream):
+        """r alone through its per-call C-ABI entry point on `stream`."""
+        P = self.P
+        h = ctypes.c_void_p(stream.cuda_stream)
+        if r.kind == "dcf":
+            c = P.dcf[r.size]
+            x = torch.empty(r.size, dtype=torch.int32, device=self.dev)
+            x.copy_(r.x_host, non_blocking=True)
+            out = torch.empty(r.size, dtype=torch.int32, device=self.dev)
+            rc = _lib.fn("FastFss_cuda_dcfEval")(out.data_ptr(), 4 * r.size, x.data_ptr(), 4 * r.size,
+                                                c.key.data_ptr(), c.key.numel(), c.seed.data_ptr(), 16 * r.size,
+                                                P.party, DCF_N, DCF_N, 1, 4, r.size, None, 0, ctypes.byref(h))
+            keep = (x, out)
+        else:
+            c = P.spline[r.size]
+            g = SPLINE_G
+            x = torch.empty(r.size, dtype=torch.int64, device=self.dev)
+            x.copy_(r.x_host, non_blocking=True)
+            out = torch.empty(r.size, dtype=torch.int64, device=self.dev)
+            csize = spline_get_cache_data_size(SPLINE_D, SPLINE_M, SPLINE_N, SPLINE_N, 8, r.size)
+            cache = torch.empty(csize, dtype=torch.uint8, device=self.dev)
+            rc = _lib.fn("FastFss_cuda_dcfSplineEval")(
+                out.data_ptr(), 8 * r.size, x.data_ptr(), 8 * r.size, c.key.data_ptr(), c.key.numel(),
+                c.e.data_ptr(), 8 * g * r.size, c.beta.data_ptr(), 8 * g * r.size, c.seed.data_ptr(), 16 * r.size,
+                P.party, P.spline_L.data_ptr(), 8 * SPLINE_M, P.spline_R.data_ptr(), 8 * SPLINE_M, SPLINE_M, SPLINE_D,
+                SPLINE_N, SPLINE_N, 8, r.size, cache.data_ptr(), csize, ctypes.byref(h))
+            keep = (x, out, cache)
+        if rc != 0:
+            raise RuntimeError(f"plain evaluation failed : {rc}")
+        r.out_host.copy_(out, non_blocking=True)
+        return keep
+
+    def run(self, requests: list[Request], mode: str = "batched", poll_s: float = 2e-5) -> float:
+        """Serves `requests` in real time; returns the makespan in seconds."""
+        pending: deque[Request] = deque()
+        arrivals = deque(sorted(requests, key=lambda r: r.arrival))
+        inflight = []  # (event, slot index or None, [requests], keep-alive)
+        free = list(range(len(self.slots)))
+        done, total = 0, len(requests)
+        t0 = time.perf_counter()
+        while done < total:
+            now = time.perf_counter() - t0
+            while arrivals and arrivals[0].arrival <= now:
+                pending.append(arrivals.popleft())
+            still = []
+            for ev, si, rs, keep in inflight:
+                if ev.query():
+                    tdone = time.perf_counter() - t0
+                    for r in rs:
+                        r.done = tdone
+                        self.store.release(r.key_bytes)
+                    done += len(rs)
+                    if si is not None:
+                        free.append(si)
+                else:
+                    still.append((ev, si, rs, keep))
+            inflight = still
+            if mode == "batched":
+                if pending and free:
+                    admitted = []
+                    while pending and self.store.try_admit(pending[0].key_bytes):
+                        admitted.append(pending.popleft())
+                    if admitted:
+                        si = free.pop()
+                        s = self.slots[si]
+                        with torch.cuda.stream(s):
+                            reqs = [self._build(r) for r in admitted]
+                            b = batch.Batch(reqs, self.dev).prepare(self.tuning)
+                            b.launch()
+                            for r, q in zip(admitted, reqs):
+                                r.out_host.copy_(q.tensors[0].view(-1), non_blocking=True)
+                            ev = torch.cuda.Event()
+                            ev.record(s)
+                        self.launches += 1
+                        tstart = time.perf_counter() - t0
+                        for r in admitted:
+                            r.start = tstart
+                        inflight.append((ev, si, admitted, (b, reqs)))
+            else:
+                s = self.slots[0]
+                while pending and self.store.try_admit(pending[0].key_bytes):
+                    r = pending.popleft()
+                    with torch.cuda.stream(s):
+                        keep = self._plain_call(r, s)
+                        ev = torch.cuda.Event()
+                        ev.record(s)
+                    self.launches += 1
+                    r.start = time.perf_counter() - t0
+                    inflight.append((ev, None, [r], keep))
+            if not (arrivals and arrivals[0].arrival <= time.perf_counter() - t0):
+                time.sleep(poll_s)
+        return time.perf_counter() - t0
+
+
+def summarize(reqs: list[Request], makespan: float) -> dict:
+    lat = np.array([(r.done - r.arrival) * 1e3 for r in reqs])
+    elems = sum(r.size for r in reqs)
+    return {"requests": len(reqs), "elements": elems, "elements_per_s": elems / makespan, "makespan_s": makespan,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean())}
+
+
+def reference_outputs(server: Server, reqs: list[Request]) -> list[np.ndarray]:
+    """Each request evaluated alone through the per-call C ABI (the alone-vs-mix check)."""
+    outs = []
+    s = torch.cuda.current_stream(server.dev)
+    for r in reqs:
+        saved = r.out_host
+        r.out_host = torch.empty_like(saved)
+        server._plain_call(r, s)
+        torch.cuda.synchronize(server.dev)
+        outs.append(r.out_host.numpy().copy())
+        r.out_host = saved
+    return outs
