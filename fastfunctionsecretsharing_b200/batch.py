@@ -122,7 +122,7 @@ class Batch:
         ws = int(_fn("FastFss_cuda_batchWorkspaceSize")(n))
         self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
         self.plan = Plan()
-        self.tuning = Tuning(256, 1 << 22, 0, 0)
+        self.tuning = Tuning(256, 1 << 26, 0, 0)
         self.elements = sum(r.elements for r in self.requests)
 
     def _stream_ref(self):
@@ -157,7 +157,7 @@ class Batch:
         return g
 
 
-DEFAULT_CANDIDATES = [Tuning(t, tl, o, 0) for t, tl, o in itertools.product((256, 512), (1 << 20, 1 << 22, 1 << 24),
+DEFAULT_CANDIDATES = [Tuning(t, tl, o, 0) for t, tl, o in itertools.product((256, 512), (1 << 24, 1 << 26, 1 << 28),
                                                                            (0, 1))]
 
 _cache: dict[tuple, Tuning] = {}

@@ -2,9 +2,10 @@
 //
 // Plan (host): every op becomes `items` work items (an element, an (element, interval) pair
 // for MIC, or a lane of a G-lane element group for spline) with an estimated cost in AES
-// table lookups per item; items are cut into tiles of about `tileLookups` lookups (a multiple
-// of 32 items, so spline groups never straddle a warp), ops are laid out costliest first and
-// numbered by a prefix sum of their tile counts.
+// table lookups per item; items are cut into tiles of about `tileLookups` lookups, in whole
+// multiples of the CTA's thread count (every thread has an item; spline lane groups never
+// straddle a warp), ops are laid out costliest first and numbered by a prefix sum of their
+// tile counts.
 //
 // Kernel (device): one CTA per SM builds the replicated AES tables once, then repeatedly
 // claims the next tile from the atomic counter in the workspace, finds its op by binary
@@ -178,7 +179,7 @@ int batch_plan(const FastFssBatchOp *ops, size_t opNum, const FastFssBatchTuning
                std::vector<BatchOpDev> &dev, FastFssBatchPlan *plan)
 {
     const uint32_t threads   = (tuning && tuning->ctaThreads == 512) ? 512u : 256u;
-    const double   tileCost  = (tuning && tuning->tileLookups) ? (double)tuning->tileLookups : (double)(1u << 22);
+    const double   tileCost  = (tuning && tuning->tileLookups) ? (double)tuning->tileLookups : (double)(1u << 26);
     const bool     callOrder = tuning && tuning->order == 1;
     struct Row
     {
@@ -202,7 +203,8 @@ int batch_plan(const FastFssBatchOp *ops, size_t opNum, const FastFssBatchTuning
         if (items == 0) continue;
         const double c  = item_cost(o, G);
         double       ti = tileCost / (c > 1 ? c : 1);
-        ti              = ti < 32 ? 32 : (ti > 1048576 ? 1048576 : ti);
+        // a tile fills every thread of the CTA at least once (whole multiples of the CTA)
+        ti = ti < threads ? threads : (ti > 1048576 ? 1048576 : ti);
         BatchOpDev d{};
         d.kind      = (uint32_t)o.kind;
         d.es        = o.elementSize;
@@ -215,7 +217,7 @@ int batch_plan(const FastFssBatchOp *ops, size_t opNum, const FastFssBatchTuning
         d.G         = G;
         d.N         = o.elementNum;
         d.items     = items;
-        d.tileItems = ((unsigned long long)ti / 32) * 32;
+        d.tileItems = ((unsigned long long)ti / threads) * threads;
         d.out       = o.sharedOut;
         d.x         = o.maskedX;
         d.key       = o.key;

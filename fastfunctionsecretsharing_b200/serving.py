@@ -182,7 +182,7 @@ class Server:
         self.dev = pools.dev
         self.store = KeyStore(capacity_bytes)
         self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
-        self.tuning = tuning or batch.Tuning(256, 1 << 21, 0, 0)
+        self.tuning = tuning or batch.Tuning(256, 1 << 26, 0, 0)
         self.launches = 0
 
     def _build(self, r: Request) -> batch.Request:

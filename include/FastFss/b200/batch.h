@@ -61,7 +61,8 @@ typedef struct FastFssBatchOp
 typedef struct FastFssBatchTuning
 {
     uint32_t ctaThreads;  /* 256 or 512; 0 selects 256 */
-    uint32_t tileLookups; /* target AES table lookups per tile; 0 selects 1 << 22 */
+    uint32_t tileLookups; /* target AES table lookups per tile (at least one item per thread);
+                             0 selects 1 << 26 */
     uint32_t order;       /* 0: costliest ops' tiles first; 1: caller order */
     uint32_t reserved;
 } FastFssBatchTuning;

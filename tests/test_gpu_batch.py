@@ -97,7 +97,7 @@ def test_graph_replay(F, oracle):
     from fastfunctionsecretsharing_b200 import batch as B
 
     reqs, want = build_mixed(oracle, np.random.default_rng(12))
-    b = B.Batch(reqs).prepare(B.Tuning(256, 1 << 20, 0, 0))
+    b = B.Batch(reqs).prepare(B.Tuning(256, 1 << 24, 0, 0))
     g = b.graph()
     for _ in range(3):
         for r in reqs:
