@@ -16,6 +16,7 @@
 #include <FastFss/errors.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "dcf_core.cuh"
@@ -305,4 +306,59 @@ extern "C" FAST_FSS_API int FastFss_cuda_batchLaunch(const FastFssBatchPlan *pla
         return FAST_FSS_RUNTIME_ERROR;
     return batch_launch(plan, reinterpret_cast<const BatchOpDev *>((char *)workspace + kBatchHeader),
                         reinterpret_cast<unsigned long long *>(workspace), resolve_stream(cudaStreamPtr));
+}
+
+// ---------------------------------------------------------------------------------------
+// No-allocation variant (FastFss_cuda_batchEvalNoAlloc in include/FastFss/b200/batch.h):
+// the work queue counter and the descriptor table live in this fixed device array instead of
+// a caller workspace. Host code must not use the array's name as a device address; it looks
+// the address up once per device with cudaGetSymbolAddress.
+// ---------------------------------------------------------------------------------------
+static_assert(sizeof(fss::BatchOpDev) == 136, "descriptor size is part of the no-alloc scratch size");
+
+static __device__ __align__(256) unsigned char g_batch_noalloc_scratch[FAST_FSS_BATCH_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void      *g_noalloc_addr[64] = {nullptr};
+
+void *noalloc_scratch_address(int device)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= 64) return nullptr;
+    if (g_noalloc_addr[device] == nullptr)
+    {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_batch_noalloc_scratch) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_noalloc_addr[device] = p;
+    }
+    return g_noalloc_addr[device];
+}
+
+} // namespace
+
+extern "C" FAST_FSS_API int FastFss_cuda_batchEvalNoAlloc(const FastFssBatchOp *ops, size_t opNum,
+                                                          const FastFssBatchTuning *tuning, void *cudaStreamPtr)
+{
+    if (opNum > FAST_FSS_BATCH_NOALLOC_MAX_OPS) return FAST_FSS_BATCH_TOO_MANY_OPS_ERROR;
+    if (opNum && ops == nullptr) return FAST_FSS_RUNTIME_ERROR;
+    std::vector<BatchOpDev> dev;
+    FastFssBatchPlan        plan{};
+    const int               rc = batch_plan(ops, opNum, tuning, dev, &plan);
+    if (rc != FAST_FSS_SUCCESS) return rc;
+    if (dev.empty()) return FAST_FSS_SUCCESS;
+    unsigned char *scratch = (unsigned char *)noalloc_scratch_address(current_device());
+    if (scratch == nullptr) return FAST_FSS_RUNTIME_ERROR;
+    cudaStream_t stream = resolve_stream(cudaStreamPtr);
+    if (cudaMemcpyAsync(scratch + kBatchHeader, dev.data(), dev.size() * sizeof(BatchOpDev), cudaMemcpyHostToDevice,
+                        stream) != cudaSuccess)
+        return FAST_FSS_RUNTIME_ERROR;
+    // batch_launch resets the queue counter (the first 8 bytes) on the stream before the kernel
+    return batch_launch(&plan, reinterpret_cast<const BatchOpDev *>(scratch + kBatchHeader),
+                        reinterpret_cast<unsigned long long *>(scratch), stream);
 }

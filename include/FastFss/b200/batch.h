@@ -85,6 +85,34 @@ FAST_FSS_API int FastFss_cuda_batchPrepare(const FastFssBatchOp *ops, size_t opN
 FAST_FSS_API int FastFss_cuda_batchLaunch(const FastFssBatchPlan *plan, void *workspace, size_t workspaceSize,
                                           void *cudaStreamPtr);
 
+/* FastFss_cuda_batchEvalNoAlloc — no counterpart in the reference.
+ *
+ * The same batched evaluation as FastFss_cuda_batchPrepare + FastFss_cuda_batchLaunch, for
+ * callers that cannot allocate device memory and have no workspace to lend: a runtime that
+ * reserves all device memory up front for its own pool (where any further cudaMalloc fails or
+ * fragments that pool), or a latency-critical loop that must not pay cudaMalloc's implicit
+ * device synchronisation. The work queue and the descriptor table live in a fixed array of
+ * device memory inside this library (FAST_FSS_BATCH_NOALLOC_SCRATCH_BYTES bytes, held by every
+ * GPU that loads the library until the process exits), so the call allocates nothing; the
+ * caller still passes every input and output buffer through the ops.
+ *
+ * Limits and behaviour:
+ *  - at most FAST_FSS_BATCH_NOALLOC_MAX_OPS ops per call; more return
+ *    FAST_FSS_BATCH_TOO_MANY_OPS_ERROR before any device work;
+ *  - the first call on a device looks up that array's device address (with the device
+ *    current); make that first call before any stream capture begins;
+ *  - every call reuses the same array: the queue counter is reset on the stream and the
+ *    descriptor table rewritten by each call, so calls that overlap on the GPU (different
+ *    streams, or different host threads without ordering) race and must not be issued;
+ *  - the call returns once the descriptor table has been staged for upload, which waits for
+ *    work already queued on the stream; validation and results as FastFss_cuda_batchPrepare. */
+#define FAST_FSS_BATCH_NOALLOC_MAX_OPS       512
+#define FAST_FSS_BATCH_NOALLOC_SCRATCH_BYTES (256 + FAST_FSS_BATCH_NOALLOC_MAX_OPS * 136)
+#define FAST_FSS_BATCH_TOO_MANY_OPS_ERROR    (-32)
+
+FAST_FSS_API int FastFss_cuda_batchEvalNoAlloc(const FastFssBatchOp *ops, size_t opNum,
+                                               const FastFssBatchTuning *tuning, void *cudaStreamPtr);
+
 #ifdef __cplusplus
 }
 #endif
