@@ -408,6 +408,10 @@ def main():
         "shares_reconstruct": ok,
     }
     if not args.no_extras:
+        del key, seed0
+        torch.cuda.empty_cache()
+        line["dpf"] = dpf_section(dev, args, peak_glookups)
+        line["grotto_full_domain"] = grotto_section(dev, args, peak_glookups)
         line["batched"] = batched_section(dev, args)
         line["serving"] = serving_section(dev, args)
     if not args.no_cpu_baseline:
@@ -415,6 +419,128 @@ def main():
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _timed(fn, dev, steps, warmup=3):
+    """Mean device ms of fn over `steps` calls on the current stream, after `warmup` calls."""
+    import torch
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / steps
+
+
+# DPF evaluation per element at n = 32, groupSize 1, 32-bit output: per level one key schedule
+# (40 lookups) and the path child's block (160); the leaf convert is one key schedule and one
+# block of which a 32-bit output reads 4 of the 16 last-round bytes (40 + 148).
+DPF_LOOKUPS_PER_ELEM = N_BITS * 200 + 40 + 148
+
+
+def dpf_section(dev, args, peak_glookups) -> dict:
+    """Plain DPF eval, 2^24 elements, n = 32 over Z_2^32 (uint32), groupSize 1, one party per
+    step; keys 16 B x 32 sCW + tCW + lastCW per element, larger than L2."""
+    import torch
+
+    import fastfunctionsecretsharing_b200 as F
+
+    N = args.elements
+    gen = torch.Generator(device=dev).manual_seed(4321)
+    alpha = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    beta = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    s0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    s1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    x = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    x[: N // 16] = 0  # a sixteenth of the points hit alpha
+    masked = x + alpha
+    key = torch.empty(0, dtype=torch.uint8, device=dev)
+    F.dpf_key_gen(key, alpha, beta, s0, s1, N_BITS, N_BITS, 1)
+    y0 = torch.empty(0, dtype=torch.int32, device=dev)
+    y1 = torch.empty(0, dtype=torch.int32, device=dev)
+    ms = _timed(lambda: F.dpf_eval(y0, masked, key, s0, 0, N_BITS, N_BITS, 1), dev, max(3, min(args.steps, 10)))
+    F.dpf_eval(y1, masked, key, s1, 1, N_BITS, N_BITS, 1)
+    ok = bool(torch.equal((y0 + y1).view(-1), torch.where(x == 0, beta, torch.zeros_like(beta))))
+    key_bytes = key.numel()
+    del alpha, beta, s0, s1, x, masked, key, y0, y1
+    torch.cuda.empty_cache()
+    ach = DPF_LOOKUPS_PER_ELEM * N / (ms / 1e3) / 1e9
+    return {"workload": "plain DPF eval, 2^24 elements, n=32, Z_2^32 (uint32), groupSize 1, one party per step",
+            "elements": N, "kernel_ms": ms, "value": N / (ms / 1e3) / 1e9, "unit": "Gelem/s",
+            "aes_blocks_per_s": (N_BITS + 1) * N / (ms / 1e3), "key_bytes_per_element": key_bytes / N,
+            "hbm_gbs": (key_bytes + N * (16 + 4 + 4)) / (ms / 1e3) / 1e9,
+            "roofline": {"bound": "smem", "achieved": ach, "peak": peak_glookups, "unit": "Glookup/s",
+                         "frac": ach / peak_glookups, "algorithmic_lookups_per_element": DPF_LOOKUPS_PER_ELEM},
+            "shares_reconstruct": ok}
+
+
+def grotto_section(dev, args, peak_glookups) -> dict:
+    """Grotto full domain over Z_2: 2^16 keys at n = 16 expanded to 2^16 leaf bits each (equality
+    rows and prefix-parity comparison rows, bit-packed), then a 64-segment lookup table (sorted
+    random boundaries, 16-bit values) evaluated from the comparison rows with warp ballots and
+    population counts; the same table through per-interval tree walks for comparison."""
+    import numpy as np
+    import torch
+
+    import fastfunctionsecretsharing_b200 as F
+    from fastfunctionsecretsharing_b200 import workloads as W
+
+    n, es, N, m = 16, 2, 1 << 16, 64
+    gen = torch.Generator(device=dev).manual_seed(99)
+    rng = np.random.default_rng(99)
+    alpha = torch.randint(-2**15, 2**15, (N,), dtype=torch.int16, device=dev, generator=gen)
+    s0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    s1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    x = torch.randint(-2**15, 2**15, (N,), dtype=torch.int16, device=dev, generator=gen)
+    masked = x + alpha
+    key = torch.empty(0, dtype=torch.uint8, device=dev)
+    F.grotto_key_gen(key, alpha, s0, s1, n)
+    L, R = W.partition(rng, m, n)
+    Lt, Rt = W._ring_tensor(L, es, dev), W._ring_tensor(R, es, dev)
+    lut = torch.randint(-2**15, 2**15, (m,), dtype=torch.int16, device=dev, generator=gen)
+    rows = torch.empty(N * ((1 << n) // 8), dtype=torch.uint8, device=dev)
+    rows1 = torch.empty_like(rows)
+    steps = max(3, min(args.steps, 10))
+    e = [torch.empty(0, dtype=torch.int16, device=dev) for _ in range(4)]
+    t = [torch.empty(0, dtype=torch.int16, device=dev) for _ in range(4)]
+
+    eq_ms = _timed(lambda: F.grotto_eq_eval_all(rows, key, s0, 0, n, es, N), dev, steps)
+    le_ms = _timed(lambda: F.grotto_le_eval_all(rows, key, s0, 0, n, es, N), dev, steps)
+    lut_rows_ms = _timed(lambda: F.grotto_interval_lut_eval_from_rows(e[0], t[0], masked, rows, 0, Lt, Rt, lut, n),
+                         dev, steps)
+    walk_ms = _timed(lambda: F.grotto_interval_lut_eval(e[1], t[1], masked, key, s0, 0, Lt, Rt, lut, n, n), dev,
+                     steps)
+    same_as_walks = bool(torch.equal(e[0], e[1]) and torch.equal(t[0], t[1]))
+    # party 1, then reconstruction as the reference's tests do it: E = E0 + E1 is +-1 (one
+    # segment holds x), T = T0 + T1, and E * T = lut[segment of x]
+    F.grotto_le_eval_all(rows1, key, s1, 1, n, es, N)
+    F.grotto_interval_lut_eval_from_rows(e[2], t[2], masked, rows1, 1, Lt, Rt, lut, n)
+    xs = x.to(torch.int64) & 0xFFFF
+    seg = torch.searchsorted(torch.tensor(R, dtype=torch.int64, device=dev), xs)
+    E = (e[0] + e[2]).view(-1)
+    ok = bool((E.abs() == 1).all() and torch.equal(E * (t[0] + t[2]).view(-1), lut[seg]))
+    del rows, rows1, key
+    torch.cuda.empty_cache()
+    D = n - 6
+    nodes = (1 << D) - 1
+    lookups_per_key = nodes * (40 + 320)
+    ach = lookups_per_key * N / (le_ms / 1e3) / 1e9
+    total = le_ms + lut_rows_ms
+    return {"workload": ("Grotto full domain over Z_2: 2^16 keys, n=16 (2^16 leaf bits per key, bit-packed), then "
+                         "a 64-segment LUT (sorted random boundaries, 16-bit values) by prefix parity"),
+            "keys": N, "eq_rows_ms": eq_ms, "le_rows_ms": le_ms, "lut_from_rows_ms": lut_rows_ms,
+            "lut_total_ms": total, "lut_by_walks_ms": walk_ms,
+            "keys_per_s": N / (total / 1e3), "leaf_bits_per_s": N * (1 << n) / (le_ms / 1e3),
+            "rows_gbs": N * (1 << n) / 8 / (le_ms / 1e3) / 1e9,
+            "roofline_rows": {"bound": "smem", "achieved": ach, "peak": peak_glookups, "unit": "Glookup/s",
+                              "frac": ach / peak_glookups, "algorithmic_lookups_per_key": lookups_per_key},
+            "lut_same_as_walks": same_as_walks, "shares_reconstruct": ok}
 
 
 def batched_section(dev, args) -> dict:

@@ -24,7 +24,7 @@ __all__ = [
     "dcf_get_key_data_size", "dcf_key_gen", "dcf_eval",
     "dpf_get_key_data_size", "dpf_key_gen", "dpf_eval", "dpf_eval_all", "dpf_multi_eval",
     "grotto_get_key_data_size", "grotto_key_gen", "grotto_eq_eval", "grotto_eval", "grotto_mic_eval",
-    "grotto_interval_lut_eval", "grotto_eq_eval_all", "grotto_le_eval_all",
+    "grotto_interval_lut_eval", "grotto_eq_eval_all", "grotto_le_eval_all", "grotto_interval_lut_eval_from_rows",
     "dcf_mic_get_key_data_size", "dcf_mic_key_gen", "dcf_mic_eval",
     "spline_get_key_data_size", "spline_key_gen", "spline_eval",
     "ottt_get_key_data_size", "ottt_key_gen", "ottt_lut_eval",
@@ -278,6 +278,24 @@ def grotto_le_eval_all(outBits, key, seed, partyId, bitWidthIn, elementSize, ele
     """Full-domain prefix-parity shares: bit x of row i is grottoEval(key_i, x, equalBound=true)."""
     return _grotto_all("FastFss_cuda_grottoLeEvalAll", outBits, key, seed, partyId, bitWidthIn, elementSize,
                        elementNum)
+
+
+def grotto_interval_lut_eval_from_rows(sharedOutE, sharedOutT, maskedX, leRows, partyId, leftBoundary,
+                                       rightBoundary, lookUpTable, bitWidthIn):
+    """grotto_interval_lut_eval computed from full-domain comparison rows (grotto_le_eval_all
+    output for the same keys/seeds/party): same shares, no tree walks."""
+    dev = _cuda(sharedOutE, sharedOutT, maskedX, leRows, leftBoundary, rightBoundary, lookUpTable)
+    es, N = maskedX.element_size(), maskedX.numel()
+    m = leftBoundary.numel()
+    lut_num = lookUpTable.numel() // m if m else 0
+    sharedOutE.resize_(maskedX.shape)
+    sharedOutT.resize_(list(maskedX.shape) + [lut_num])
+    st = _Stream(dev)
+    _check("FastFss_cuda_grottoIntervalLutEvalFromRows", _lib.fn("FastFss_cuda_grottoIntervalLutEvalFromRows")(
+        _ptr(sharedOutE), _nbytes(sharedOutE), _ptr(sharedOutT), _nbytes(sharedOutT), _ptr(maskedX), _nbytes(maskedX),
+        _ptr(leRows), _nbytes(leRows), partyId, _ptr(leftBoundary), _nbytes(leftBoundary), _ptr(rightBoundary),
+        _nbytes(rightBoundary), _ptr(lookUpTable), _nbytes(lookUpTable), bitWidthIn, es, N, st.ptr))
+    return sharedOutE, sharedOutT
 
 
 # ------------------------------------------------------------------------------------

@@ -93,6 +93,9 @@ EXTENSION_SIGNATURES: dict[str, tuple] = {
     "FastFss_b200_smCount": (_I, []),
     "FastFss_cuda_grottoEqEvalAll": (_I, [_P, _S, _P, _S, _P, _S, _I, _S, _S, _S, _P]),
     "FastFss_cuda_grottoLeEvalAll": (_I, [_P, _S, _P, _S, _P, _S, _I, _S, _S, _S, _P]),
+    "FastFss_cuda_grottoIntervalLutEvalFromRows": (
+        _I, [_P, _S, _P, _S, _P, _S, _P, _S, _I, _P, _S, _P, _S, _P, _S, _S, _S, _S, _P]),
+    "FastFss_cuda_batchEvalNoAlloc": (_I, [_P, _S, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -190,6 +190,57 @@ __device__ __forceinline__ void aes_encrypt(const AesLanes& A, const uint32_t ke
     for (int b = 0; b < NB; b++) enc_last(A, st[b], w);
 }
 
+// NK independent keys, NB blocks under each. The round loop is not unrolled (small code for
+// the kernels that instantiate several of these); inside an iteration the block rounds under
+// round key r and the schedule step to round key r + 1 are independent, so they overlap.
+template <int NK, int NB>
+__device__ __forceinline__ void aes_encrypt_keys(const AesLanes& A, const uint32_t key[NK][4],
+                                                 uint32_t st[NK][NB][4])
+{
+    uint32_t w[NK][4];
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) w[k][c] = key[k][c];
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) st[k][b][c] ^= w[k][c];
+        }
+        key_step(A, w[k], 0x01u);
+    }
+    uint32_t rcon = 0x01u;
+#pragma unroll 1
+    for (int r = 1; r < 10; r++)
+    {
+        rcon = gf_xtime(rcon);
+        uint32_t nw[NK][4];
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) nw[k][c] = w[k][c];
+            key_step(A, nw[k], rcon);
+#pragma unroll
+            for (int b = 0; b < NB; b++) enc_round(A, st[k][b], w[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) w[k][c] = nw[k][c];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+#pragma unroll
+        for (int b = 0; b < NB; b++) enc_last(A, st[k][b], w[k]);
+    }
+}
+
 // PRG block j of the GGM expansion: plaintext = LE64(2j) || LE64(2j+1) as BE words.
 __device__ __forceinline__ void prg_block(uint32_t st[4], uint32_t j)
 {

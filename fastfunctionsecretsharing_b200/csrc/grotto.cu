@@ -303,6 +303,64 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
     }
 }
 
+// Interval LUT from comparison rows: one warp per element, lanes stride over the intervals.
+template <typename GE, int LMAX>
+__global__ void __launch_bounds__(256)
+    grotto_lut_rows_kernel(GE *__restrict__ outE, GE *__restrict__ outT, const GE *__restrict__ maskedX,
+                           const uint8_t *__restrict__ rows, uint32_t party, const GE *__restrict__ left,
+                           const GE *__restrict__ right, const GE *__restrict__ lut, uint32_t lutNum, uint32_t m,
+                           uint32_t n, size_t N, uint32_t j0)
+{
+    const uint32_t lane  = threadIdx.x & 31u;
+    const size_t   warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t   rowBytes = ((size_t)1 << n) >> 3;
+    const uint32_t jcnt  = lutNum > j0 ? min((uint32_t)LMAX, lutNum - j0) : 0u;
+    for (size_t i = (((size_t)blockIdx.x * blockDim.x) + threadIdx.x) >> 5; i < N; i += warps)
+    {
+        const uint8_t *row = rows + i * rowBytes;
+        const uint64_t x   = (uint64_t)__ldg(maskedX + i);
+        uint32_t       E   = 0;
+        uint64_t       T[LMAX];
+#pragma unroll
+        for (int k = 0; k < LMAX; k++) T[k] = 0;
+        for (uint32_t q0 = 0; q0 < m; q0 += 32)
+        {
+            const uint32_t q   = q0 + lane;
+            uint32_t       bit = 0;
+            if (q < m)
+            {
+                const uint64_t L  = (uint64_t)__ldg(left + q), R = (uint64_t)__ldg(right + q);
+                const uint64_t xP = mod_bits<GE>((uint64_t)(GE)(x - (uint64_t)(GE)(L - 1)), n);
+                const uint64_t xQ = mod_bits<GE>((uint64_t)(GE)(x - R), n);
+                const uint32_t sp = (__ldg(row + (xP >> 3)) >> (xP & 7)) & 1u;
+                const uint32_t sq = (__ldg(row + (xQ >> 3)) >> (xQ & 7)) & 1u;
+                bit               = (sp ^ sq ^ ((xQ >= xP) ? party : 0u)) & 1u;
+#pragma unroll
+                for (int k = 0; k < LMAX; k++)
+                    if ((uint32_t)k < jcnt) T[k] += bit * (uint64_t)__ldg(lut + q + (size_t)(j0 + k) * m);
+            }
+            E += __popc(__ballot_sync(0xffffffffu, bit));
+        }
+#pragma unroll
+        for (int k = 0; k < LMAX; k++)
+            for (uint32_t off = 16; off > 0; off >>= 1) T[k] += __shfl_xor_sync(0xffffffffu, T[k], off);
+        if (lane == 0)
+        {
+            uint64_t e = E;
+            if (party)
+            {
+                e = 0 - e;
+#pragma unroll
+                for (int k = 0; k < LMAX; k++) T[k] = 0 - T[k];
+            }
+            if (j0 == 0) outE[i] = (GE)e;
+#pragma unroll
+            for (int k = 0; k < LMAX; k++)
+                if ((uint32_t)k < jcnt) outT[i * lutNum + j0 + k] = (GE)T[k];
+        }
+    }
+}
+
 static inline size_t grotto_key_bytes(size_t n, size_t es, size_t N)
 {
     return N * (16 * (n - 6) + 8 + 2 * es);
@@ -514,4 +572,40 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoLeEvalAll(void *outBits, size_t o
 {
     return grotto_all_entry<1>(outBits, outBitsDataSize, key, keyDataSize, seed, seedDataSize, partyId, bitWidthIn,
                                elementSize, elementNum, cudaStreamPtr);
+}
+
+// Validation follows FastFss_cuda_grottoIntervalLutEval, with the rows in place of the key.
+extern "C" FAST_FSS_API int FastFss_cuda_grottoIntervalLutEvalFromRows(
+    void *sharedOutE, size_t sharedOutEDataSize, void *sharedOutT, size_t sharedOutTDataSize, const void *maskedX,
+    size_t maskedXDataSize, const void *leRows, size_t leRowsDataSize, int partyId, const void *leftEndpoints,
+    size_t leftEndpointsDataSize, const void *rightEndpoints, size_t rightEndpointsDataSize, const void *lookUpTable,
+    size_t lookUpTableDataSize, size_t bitWidthIn, size_t elementSize, size_t elementNum, void *cudaStreamPtr)
+{
+    return dispatch_es(elementSize, [&](auto tag) -> int {
+        using GE        = decltype(tag);
+        const size_t es = sizeof(GE), N = elementNum, n = bitWidthIn;
+        if (!(6 <= n && n <= es * 8 && n <= FAST_FSS_GROTTO_ALL_MAX_BITWIDTH)) return FAST_FSS_INVALID_BITWIDTH_ERROR;
+        if (!(leftEndpointsDataSize == rightEndpointsDataSize && leftEndpointsDataSize % es == 0))
+            return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
+        const size_t m = leftEndpointsDataSize / es;
+        if (m == 0 || lookUpTableDataSize % (es * m) != 0) return FAST_FSS_INVALID_LOOKUP_TABLE_DATA_SIZE_ERROR;
+        const size_t lutNum = lookUpTableDataSize / (es * m);
+        if (sharedOutEDataSize != N * es) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (sharedOutTDataSize != N * es * lutNum) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
+        if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
+        if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
+        if (leRowsDataSize != N * (((size_t)1 << n) / 8)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
+        if (N == 0) return FAST_FSS_SUCCESS;
+        cudaStream_t  stream = resolve_stream(cudaStreamPtr);
+        constexpr int LMAX   = 4;
+        for (size_t j0 = 0; j0 < (lutNum ? lutNum : 1); j0 += LMAX)
+        {
+            grotto_lut_rows_kernel<GE, LMAX><<<grid_for(N * 32, 256, 8), 256, 0, stream>>>(
+                (GE *)sharedOutE, (GE *)sharedOutT, (const GE *)maskedX, (const uint8_t *)leRows, (uint32_t)partyId,
+                (const GE *)leftEndpoints, (const GE *)rightEndpoints, (const GE *)lookUpTable, (uint32_t)lutNum,
+                (uint32_t)m, (uint32_t)n, N, (uint32_t)j0);
+            if (launch_status() != FAST_FSS_SUCCESS) return FAST_FSS_RUNTIME_ERROR;
+        }
+        return FAST_FSS_SUCCESS;
+    });
 }

@@ -9,8 +9,8 @@
 // only interval q's d + 1 values of it (src/impl/spline.h:226-249). Here each interval is
 // handled by its own lane of a G-lane group, which walks the two DCF paths of interval q
 // (x - 1 - L_q and x - 1 - (R_q + 1)) and reads only slot q's values out of each level's
-// convert stream: AES-CTR blocks of the stream are produced on demand, so a level costs one
-// extra key schedule and the one or two blocks holding slot q (not ceil(16 g / 16) blocks).
+// convert stream: the AES-CTR blocks holding slot q are produced under one extra key schedule
+// per level (not all ceil(ges g / 16) blocks of the stream).
 // Coefficient sums are reduced across the group with warp shuffles and lane 0 evaluates the
 // polynomial. Shares are bit-identical to the reference; nothing is written to the cache.
 #include <FastFss/cuda/spline.h>
@@ -23,7 +23,8 @@
 
 namespace fss {
 
-constexpr int kSplineThreads = 256;
+constexpr int kSplineThreads     = 256; // key generation
+constexpr int kSplineEvalThreads = 512; // evaluation: 16 warps per SM at <= 128 registers
 
 // splineShiftPolynomialCoefficients (src/impl/spline.h:89-117), writing d + 1 values.
 template <typename GE>
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(kSplineThreads, 1)
 }
 
 template <typename GE>
-__global__ void __launch_bounds__(kSplineThreads, 1)
+__global__ void __launch_bounds__(kSplineEvalThreads, 1)
     spline_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
                        const GE *__restrict__ sharedE, const GE *__restrict__ sharedBeta,
                        const uint8_t *__restrict__ seed, uint32_t party, const GE *__restrict__ left,
@@ -172,7 +173,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfSplineEval(
         while (G < 32 && G < m) G <<= 1;
         auto kern = spline_eval_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N * G, kSplineThreads, 1), kSplineThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
+        kern<<<grid_for(N * G, kSplineEvalThreads, 1), kSplineEvalThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
             (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const GE *)sharedE, (const GE *)sharedBeta,
             (const uint8_t *)seed, (uint32_t)partyId, (const GE *)leftEndpoints, (const GE *)rightEndpoints,
             (uint32_t)m, (uint32_t)degree, (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, N, G);

@@ -1,6 +1,13 @@
 // spline_core.cuh — one element's DCF-spline evaluation by a group of G lanes (G a power of two
 // <= 32, all lanes of a warp call it together), shared by the spline kernel and the batched
 // persistent kernel. Algorithm: src/impl/spline.h:186-253 of the reference.
+//
+// Lane lg of element i takes intervals q = lg, lg + G, ... . For interval q it walks the two
+// DCF paths x - 1 - L_q and x - 1 - (R_q + 1) side by side (one AES call carries both paths'
+// blocks, so a level issues twice the independent lookups), and reads only slot q's values
+// out of each level's convert stream: the value bytes j0 ges .. (j0 + cnt) ges - 1 lie in at
+// most three consecutive 16-byte blocks of the AES-CTR stream, which are encrypted under one
+// key schedule and read with register masks (no dynamically indexed arrays).
 #pragma once
 
 #include "dcf_core.cuh"
@@ -9,10 +16,156 @@ namespace fss {
 
 constexpr int kSplineMaxC = 4; // coefficients reduced per pass
 
-// Lane lg of element i walks intervals q = lg, lg + G, ...: both DCF paths of interval q,
-// reading only slot q's d + 1 values out of each level's convert stream, and accumulates
-// w_c += cx beta_qc - s_qc + s'_qc + e_qc. The group sums are reduced with shuffles and
-// lane 0 writes sum_c w_c x^c mod 2^bitWidthOut.
+// Little-endian 64-bit words of a window of NB blocks held as big-endian words.
+template <int NB>
+__device__ __forceinline__ void window_words(const uint32_t W[NB][4], uint64_t D[2 * NB])
+{
+#pragma unroll
+    for (int q = 0; q < 2 * NB; q++)
+        D[q] = (uint64_t)bswap32(W[q >> 1][2 * (q & 1)]) | ((uint64_t)bswap32(W[q >> 1][2 * (q & 1) + 1]) << 32);
+}
+
+// Little-endian value of the `ges` (1..8) bytes at byte offset p of the window; p + ges <= 16 NB.
+template <int NB>
+__device__ __forceinline__ uint64_t window_value(const uint64_t D[2 * NB], uint32_t p, uint32_t ges)
+{
+    const uint32_t j = p >> 3, sh = 8u * (p & 7u);
+    uint64_t       lo = 0, hi = 0;
+    // masks rather than selects: a select chain over D is turned into a local-memory array
+#pragma unroll
+    for (int q = 0; q < 2 * NB; q++)
+    {
+        lo ^= D[q] & (0ull - (uint64_t)((uint32_t)q == j));
+        hi ^= D[q] & (0ull - (uint64_t)((uint32_t)q == j + 1));
+    }
+    const uint64_t v = sh ? ((lo >> sh) | (hi << (64u - sh))) : lo;
+    return ges >= 8 ? v : (v & ((1ull << (8u * ges)) - 1ull));
+}
+
+// Blocks of the convert stream needed for values j0 .. j0 + cnt - 1 of every interval, the
+// same for all lanes: the maximum over the intervals' start offsets (period 16 in q).
+__device__ __forceinline__ uint32_t spline_window_blocks(uint32_t m, uint32_t cn, uint32_t c0, uint32_t cnt,
+                                                         uint32_t ges)
+{
+    uint32_t nb = 1;
+    for (uint32_t q = 0; q < m && q < 16; q++)
+    {
+        const uint32_t off = ((q * cn + c0) * ges) & 15u;
+        nb                 = max(nb, (off + cnt * ges + 15u) >> 4);
+    }
+    return nb;
+}
+
+// Adds the shares of values j0 .. j0 + cnt - 1 of the two convert streams keyed by key[0] and
+// key[1] (with the correction corr[j0 + c] where tc[k] is set) into acc[k][c].
+template <typename GE, int NB, bool AES>
+__device__ __forceinline__ void spline_slot_add(const AesLanes &A, const uint32_t key[2][4], const uint32_t tc[2],
+                                                const GE *corr, uint32_t party, uint32_t ges, uint32_t off,
+                                                const uint32_t ctr[NB], uint32_t j0, uint32_t cnt,
+                                                uint64_t acc[2][kSplineMaxC])
+{
+    uint32_t W[2][NB][4];
+    if (AES)
+    {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+            {
+                W[k][b][0] = 0;
+                W[k][b][1] = 0;
+                W[k][b][2] = bswap32(ctr[b]);
+                W[k][b][3] = 0;
+            }
+        }
+        aes_encrypt_keys<2, NB>(A, key, W);
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) W[k][0][c] = key[k][c];
+        }
+    }
+    uint64_t cv[kSplineMaxC];
+#pragma unroll
+    for (int c = 0; c < kSplineMaxC; c++) cv[c] = ((uint32_t)c < cnt) ? (uint64_t)__ldg(corr + j0 + c) : 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+    {
+        uint64_t D[2 * NB];
+        window_words<NB>(W[k], D);
+#pragma unroll
+        for (int c = 0; c < kSplineMaxC; c++)
+        {
+            if ((uint32_t)c < cnt)
+            {
+                const uint64_t val = window_value<NB>(D, off + (uint32_t)c * ges, ges) + (tc[k] ? cv[c] : 0);
+                acc[k][c] += party ? (0 - val) : val;
+            }
+        }
+    }
+}
+
+// Both DCF walks of one interval (points xa, xb), slot values j0 .. j0 + cnt - 1.
+template <typename GE, int NB, bool AES>
+__device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
+                                                 uint32_t party, uint32_t n, uint32_t g, uint32_t ges, uint64_t xa,
+                                                 uint64_t xb, uint32_t j0, uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+{
+    const uint32_t start = j0 * ges;
+    const uint32_t blo   = AES ? (start >> 4) : 0u;
+    const uint32_t off   = start - 16u * blo;
+    uint32_t       ctr[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) ctr[b] = (16u * (blo + (uint32_t)b)) / ges;
+    uint32_t s[2][4];
+    load_block_be(seed, s[0]);
+    s[0][0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++) s[1][c] = s[0][c];
+    uint32_t t[2] = {party, party};
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        uint32_t cw[4];
+        load_block_be(K.sCW + 16 * lv, cw);
+        const uint32_t dir[2] = {(uint32_t)((xa >> (n - 1 - lv)) & 1u), (uint32_t)((xb >> (n - 1 - lv)) & 1u)};
+        uint32_t       st[2][2][4];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            prg_block(st[k][0], 2 * dir[k]);
+            prg_block(st[k][1], 2 * dir[k] + 1);
+        }
+        aes_encrypt_keys<2, 2>(A, s, st);
+        uint32_t v[2][4], tp[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            tp[k]            = t[k];
+            uint32_t       tn = (st[k][0][0] >> 24) & 1u;
+            const uint32_t mk = 0u - t[k];
+            st[k][0][0] &= ~kSeedTBit;
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+            {
+                s[k][c] = st[k][0][c] ^ (cw[c] & mk);
+                v[k][c] = st[k][1][c];
+            }
+            tn ^= (uint32_t)(((dir[k] ? K.tr : K.tl) >> lv) & 1u) & t[k];
+            t[k] = tn;
+        }
+        spline_slot_add<GE, NB, AES>(A, v, tp, K.vCW + (size_t)lv * g, party, ges, off, ctr, j0, cnt, acc);
+    }
+    spline_slot_add<GE, NB, AES>(A, s, t, K.last, party, ges, off, ctr, j0, cnt, acc);
+}
+
+// The group sums w_c += cx beta_qc - s_qc + s'_qc + e_qc are reduced with shuffles and lane 0
+// writes sum_c w_c x^c mod 2^bitWidthOut.
 template <typename GE>
 __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, const GE *maskedX, const uint8_t *key,
                                                   const GE *sharedE, const GE *sharedBeta, const uint8_t *seed,
@@ -21,6 +174,8 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
                                                   uint32_t lg, bool active)
 {
     const uint32_t cn = d + 1, g = m * cn;
+    const uint32_t ges = (bo + 7) / 8;
+    const bool     aes = (uint64_t)ges * g > 16; // convert keyed stream (src/impl/dcf.h:69-137)
     DcfKeyView<GE> K;
     uint64_t       x = 0;
     if (active)
@@ -32,6 +187,7 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
     for (uint32_t c0 = 0; c0 < cn; c0 += kSplineMaxC)
     {
         const uint32_t cnt = min((uint32_t)kSplineMaxC, cn - c0);
+        const uint32_t nb  = aes ? spline_window_blocks(m, cn, c0, cnt, ges) : 1u;
         uint64_t       acc[kSplineMaxC];
 #pragma unroll
         for (int k = 0; k < kSplineMaxC; k++) acc[k] = 0;
@@ -42,13 +198,21 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
                 const uint64_t L  = mod_bits<GE>((uint64_t)__ldg(left + q), n);
                 const uint64_t R  = mod_bits<GE>((uint64_t)__ldg(right + q), n);
                 const uint64_t Rp = mod_bits<GE>((uint64_t)(GE)(R + 1), n);
-                uint64_t       sL[kSplineMaxC], sR[kSplineMaxC];
+                const uint64_t xa = mod_bits<GE>((uint64_t)(GE)(x - 1 - L), n);
+                const uint64_t xb = mod_bits<GE>((uint64_t)(GE)(x - 1 - Rp), n);
+                const uint32_t j0 = q * cn + c0;
+                uint64_t       w[2][kSplineMaxC];
 #pragma unroll
-                for (int k = 0; k < kSplineMaxC; k++) sL[k] = 0, sR[k] = 0;
-                dcf_eval_slice<GE, kSplineMaxC>(A, sL, K, seed + 16 * i, party, n, bo, g,
-                                                mod_bits<GE>((uint64_t)(GE)(x - 1 - L), n), q * cn + c0, cnt);
-                dcf_eval_slice<GE, kSplineMaxC>(A, sR, K, seed + 16 * i, party, n, bo, g,
-                                                mod_bits<GE>((uint64_t)(GE)(x - 1 - Rp), n), q * cn + c0, cnt);
+                for (int k = 0; k < kSplineMaxC; k++) w[0][k] = 0, w[1][k] = 0;
+                const uint8_t *sd = seed + 16 * i;
+                if (!aes)
+                    spline_walk_pair<GE, 1, false>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);
+                else if (nb == 1)
+                    spline_walk_pair<GE, 1, true>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);
+                else if (nb == 2)
+                    spline_walk_pair<GE, 2, true>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);
+                else
+                    spline_walk_pair<GE, 3, true>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);
                 const uint64_t cx = (uint64_t)((int64_t)(x > L) - (int64_t)(x > Rp));
 #pragma unroll
                 for (int k = 0; k < kSplineMaxC; k++)
@@ -57,7 +221,7 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
                     {
                         const size_t   o = i * g + q * cn + c0 + k;
                         const uint64_t b = (uint64_t)__ldg(sharedBeta + o);
-                        acc[k] += cx * b - sL[k] + sR[k] + (uint64_t)__ldg(sharedE + o);
+                        acc[k] += cx * b - w[0][k] + w[1][k] + (uint64_t)__ldg(sharedE + o);
                     }
                 }
             }

@@ -32,6 +32,18 @@ FAST_FSS_API int FastFss_cuda_grottoLeEvalAll(void *outBits, size_t outBitsDataS
                                               size_t bitWidthIn, size_t elementSize, size_t elementNum,
                                               void *cudaStreamPtr);
 
+/* Interval lookup table from full-domain comparison rows (no counterpart in the reference;
+ * BASELINE config 3's prefix-parity path). leRows is the output of FastFss_cuda_grottoLeEvalAll
+ * for the same keys, seeds and party; the shares written are exactly those of
+ * FastFss_cuda_grottoIntervalLutEval on the same inputs: for interval q the endpoint bits
+ * sp = row[(x - (L_q - 1)) mod 2^n], sq = row[(x - R_q) mod 2^n] replace the two tree walks.
+ * One warp per element; E is a ballot population count per 32 intervals, T_j a shuffle sum. */
+FAST_FSS_API int FastFss_cuda_grottoIntervalLutEvalFromRows(
+    void *sharedOutE, size_t sharedOutEDataSize, void *sharedOutT, size_t sharedOutTDataSize, const void *maskedX,
+    size_t maskedXDataSize, const void *leRows, size_t leRowsDataSize, int partyId, const void *leftEndpoints,
+    size_t leftEndpointsDataSize, const void *rightEndpoints, size_t rightEndpointsDataSize, const void *lookUpTable,
+    size_t lookUpTableDataSize, size_t bitWidthIn, size_t elementSize, size_t elementNum, void *cudaStreamPtr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -156,3 +156,23 @@ def test_full_domain_config3_reconstruction(F):
     for b in range(8):
         cnt += ((le >> b) & 1).sum(dim=1)
     assert torch.equal(cnt, av + 1)
+
+
+@pytest.mark.parametrize("es,n,m,lutn", [(2, 16, 64, 1), (2, 10, 5, 6), (4, 20, 40, 2), (1, 8, 3, 1)])
+def test_lut_from_rows_equals_walks(F, oracle, es, n, m, lutn):
+    """The prefix-parity path (full-domain rows, then the LUT from rows) gives the shares of
+    the walk-based interval LUT, which are the reference's."""
+    rng = np.random.default_rng(n * 7 + m)
+    N = 200
+    a, s0, s1 = rnd(rng, N, es, n), seeds(rng, N), seeds(rng, N)
+    kref = oracle.grotto_keygen(a, s0, s1, n)
+    x = rnd(rng, N, es, 8 * es)
+    L, R = sorted_partition(rng, m, es, n)
+    lut = rnd(rng, m * lutn, es, 8 * es)
+    for p, s in ((0, s0), (1, s1)):
+        rows = empty_bytes()
+        F.grotto_le_eval_all(rows, dev_bytes(kref), dev_bytes(s), p, n, es, N)
+        oe, ot = empty_ring(es), empty_ring(es)
+        F.grotto_interval_lut_eval_from_rows(oe, ot, dev_ring(x), rows, p, dev_ring(L), dev_ring(R), dev_ring(lut), n)
+        we, wt = oracle.grotto_interval_lut_eval(x, kref, s, p, L, R, lut, n, 8 * es)
+        assert np.array_equal(host(oe, es), we) and np.array_equal(host(ot, es), wt)

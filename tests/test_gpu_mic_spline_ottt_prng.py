@@ -77,7 +77,8 @@ def test_spline_golden(F, name):
 
 
 @pytest.mark.parametrize("es,n,bo,m,d", [(8, 64, 64, 32, 2), (2, 16, 16, 7, 1), (4, 32, 24, 4, 5), (1, 8, 8, 3, 0),
-                                         (8, 48, 64, 2, 8)])
+                                         (8, 48, 64, 2, 8), (8, 40, 40, 5, 1), (8, 64, 56, 3, 3), (4, 32, 32, 2, 0),
+                                         (2, 12, 12, 5, 2), (4, 32, 32, 9, 2), (8, 64, 64, 1, 0)])
 def test_spline_vs_oracle(F, oracle, es, n, bo, m, d):
     rng = np.random.default_rng(zlib.crc32(repr(("spline", es, n, bo, m, d)).encode()))
     N = 40
