@@ -67,7 +67,9 @@ def parse():
     ap.add_argument("--elements", type=int, default=N_ELEMENTS)
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="wall budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the DPF, Grotto, batched and serving measurements")
+    ap.add_argument("--sections", default="dpf,grotto,batched,serving",
+                    help="comma-separated extra measurements to run after the DCF line")
     ap.add_argument("--batched-instances", type=int, default=256)
     ap.add_argument("--serving-requests", type=int, default=160)
     return ap.parse_args()
@@ -410,10 +412,15 @@ def main():
     if not args.no_extras:
         del key, seed0
         torch.cuda.empty_cache()
-        line["dpf"] = dpf_section(dev, args, peak_glookups)
-        line["grotto_full_domain"] = grotto_section(dev, args, peak_glookups)
-        line["batched"] = batched_section(dev, args)
-        line["serving"] = serving_section(dev, args)
+        sections = set(args.sections.split(","))
+        if "dpf" in sections:
+            line["dpf"] = dpf_section(dev, args, peak_glookups)
+        if "grotto" in sections:
+            line["grotto_full_domain"] = grotto_section(dev, args, peak_glookups)
+        if "batched" in sections:
+            line["batched"] = batched_section(dev, args, peak_glookups)
+        if "serving" in sections:
+            line["serving"] = serving_section(dev, args)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_rate(args.cpu_seconds)
     print(json.dumps(line), flush=True)
@@ -543,7 +550,7 @@ def grotto_section(dev, args, peak_glookups) -> dict:
             "lut_same_as_walks": same_as_walks, "shares_reconstruct": ok}
 
 
-def batched_section(dev, args) -> dict:
+def batched_section(dev, args, peak_glookups) -> dict:
     """Mixed-bitwidth MIC + spline batch: plain per-call C-ABI loop vs one persistent launch
     (autotuned, CUDA-graph captured), same instances, same stream; elements/s of both."""
     import torch
@@ -555,6 +562,7 @@ def batched_section(dev, args) -> dict:
     inst = W.mixed_mic_spline(device=dev, instances=args.batched_instances, seed=4, mic_log2=mic_log2,
                               spline_log2=spline_log2)
     elems = sum(i.N for i in inst)
+    lookups = sum(i.lookups for i in inst)
     stream = torch.cuda.current_stream(dev)
     steps = max(3, min(args.steps, 10))
 
@@ -584,7 +592,10 @@ def batched_section(dev, args) -> dict:
            "speedup": plain_ms / batched_ms, "plain_launches_per_step": len(inst),
            "batched_launches_per_step": 1, "tuning": list(best.as_tuple()),
            "autotune_ms": {str(k): v for k, v in timings.items()}, "outputs_match_plain": bool(same),
-           "estimated_lookups": b.plan.lookups}
+           "algorithmic_lookups_per_step": lookups,
+           "roofline": {"bound": "smem", "peak": peak_glookups, "unit": "Glookup/s",
+                        "plain_frac": lookups / (plain_ms / 1e3) / 1e9 / peak_glookups,
+                        "batched_frac": lookups / (batched_ms / 1e3) / 1e9 / peak_glookups}}
     del inst, b, g
     torch.cuda.empty_cache()
     return res
@@ -599,8 +610,11 @@ def serving_section(dev, args) -> dict:
     P = S.make_pools(dev, dcf_log2=(10, 20), spline_log2=(10, 14))
     out = {"workload": ("12-layer MLP (width 4096, batch 64) trace: 2^18 ReLU DCFs (n=32) + 2^18 GeLU splines "
                         "(n=64, 32 intervals, degree 2) per layer, issued as requests of 2^k elements (DCF k in "
-                        "10..20, spline k in 10..14); key store 64 GB charged per request; 4 stream slots"),
+                        "10..20, spline k in 10..14); key store 64 GB charged per request; batches capped at about "
+                        "4 ms of GPU work, at most 2 in flight on 4 stream slots; plain = one per-call C-ABI "
+                        "evaluation per request, FIFO on one stream"),
            "rates": []}
+    S.Server(P).warmup()
     for rate in (100.0, 1000.0, 10000.0):
         row = {"rate_req_per_s": rate}
         for mode in ("batched", "plain"):

@@ -5,7 +5,8 @@
 // table lookups per item; items are cut into tiles of about `tileLookups` lookups, in whole
 // multiples of the CTA's thread count (every thread has an item; spline lane groups never
 // straddle a warp), ops are laid out costliest first and numbered by a prefix sum of their
-// tile counts.
+// tile counts. A batch with fewer items than the SMs' CTAs have threads is instead cut into
+// about one tile per SM (whole warps), so small batches use every SM.
 //
 // Kernel (device): one CTA per SM builds the replicated AES tables once, then repeatedly
 // claims the next tile from the atomic counter in the workspace, finds its op by binary
@@ -16,6 +17,7 @@
 #include <FastFss/errors.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <vector>
 
@@ -229,6 +231,24 @@ int batch_plan(const FastFssBatchOp *ops, size_t opNum, const FastFssBatchTuning
         d.R         = o.rightEndpoints;
         rows.push_back({d, c});
         lookups += c * (double)items;
+    }
+    // A batch too small to give every SM a full CTA of items is spread over all SMs instead:
+    // each op gets tiles in proportion to its share of the work, down to one warp of items (the
+    // CTAs then run partly idle, on SMs that would otherwise have nothing to do).
+    unsigned long long allItems = 0;
+    for (const auto &r : rows) allItems += r.d.items;
+    const unsigned long long sms = (unsigned long long)sm_count();
+    if (!rows.empty() && allItems < sms * threads && lookups > 0)
+    {
+        for (auto &r : rows)
+        {
+            const double share = r.cost * (double)r.d.items / lookups;
+            double       want  = std::ceil(share * (double)sms);
+            want               = want < 1 ? 1 : want;
+            unsigned long long ti = (unsigned long long)std::ceil((double)r.d.items / want);
+            ti                    = ((ti + 31) / 32) * 32;
+            r.d.tileItems         = std::min<unsigned long long>(r.d.tileItems, std::max<unsigned long long>(32, ti));
+        }
     }
     if (!callOrder)
         std::stable_sort(rows.begin(), rows.end(), [](const Row &a, const Row &b) { return a.cost > b.cost; });

@@ -97,31 +97,109 @@ __device__ __forceinline__ void dcf_eval_slice(const AesLanes &A, uint64_t out[M
     }
 }
 
+// One level for groupSize 1 of NK walks under the same key (correction words shared): like
+// dcf_step, but each value child is produced only as far as its first VW words (the bytes a
+// groupSize-1 convert reads: ceil(bo / 8) <= 4 VW).
+template <int NK, int VW>
+__device__ __forceinline__ void dcf_step_g1(const AesLanes &A, uint32_t s[NK][4], uint32_t t[NK],
+                                            const uint32_t dir[NK], const uint8_t *cwp, uint64_t tl, uint64_t tr,
+                                            uint32_t lv, uint32_t v[NK][VW])
+{
+    uint32_t cw[4];
+    load_block_be(cwp, cw);
+    uint32_t sn[NK][4];
+    aes_prg_pair<NK, VW>(A, s, dir, sn, v);
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+        uint32_t       tn = (sn[k][0] >> 24) & 1u;
+        const uint32_t m  = 0u - t[k];
+        sn[k][0] &= ~kSeedTBit;
+#pragma unroll
+        for (int c = 0; c < 4; c++) s[k][c] = sn[k][c] ^ (cw[c] & m);
+        tn ^= (uint32_t)(((dir[k] ? tr : tl) >> lv) & 1u) & t[k];
+        t[k] = tn;
+    }
+}
+
+// Little-endian value of the first `nbytes` (1 .. 4 VW) bytes of a block's first VW words.
+template <int VW>
+__device__ __forceinline__ uint64_t words_le_prefix(const uint32_t w[VW], int nbytes)
+{
+    const uint64_t v = (uint64_t)bswap32(w[0]) | (VW > 1 ? ((uint64_t)bswap32(w[VW > 1 ? 1 : 0]) << 32) : 0ull);
+    return nbytes >= 8 ? v : (v & ((1ull << (8 * nbytes)) - 1ull));
+}
+
+// groupSize-1 shares of NK points x[k] under one key (the walks run side by side).
+template <typename GE, int NK, int VW>
+__device__ __forceinline__ void dcf_eval_g1_vw(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
+                                               uint32_t party, uint32_t n, uint32_t bo, const uint64_t x[NK],
+                                               uint64_t acc[NK])
+{
+    const int ges = (int)((bo + 7) / 8);
+    uint32_t  s[NK][4], t[NK];
+    load_block_be(seed, s[0]);
+    s[0][0] &= ~kSeedTBit;
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) s[k][c] = s[0][c];
+        t[k]   = party;
+        acc[k] = 0;
+    }
+#pragma unroll 1
+    for (uint32_t lv = 0; lv < n; lv++)
+    {
+        uint32_t dir[NK], tp[NK], v[NK][VW];
+#pragma unroll
+        for (int k = 0; k < NK; k++) dir[k] = (uint32_t)((x[k] >> (n - 1 - lv)) & 1u), tp[k] = t[k];
+        const uint64_t vcw = (uint64_t)__ldg(K.vCW + lv);
+        dcf_step_g1<NK, VW>(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv, v);
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+        {
+            const uint64_t val = words_le_prefix<VW>(v[k], ges) + (tp[k] ? vcw : 0);
+            acc[k] += party ? (0 - val) : val;
+        }
+    }
+    const uint64_t last = (uint64_t)__ldg(K.last);
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+        const uint64_t val = block_le_prefix(s[k], ges) + (t[k] ? last : 0);
+        acc[k] += party ? (0 - val) : val;
+    }
+}
+
 // groupSize 1 share (the convert is a plain read of the first ceil(bo/8) bytes).
 template <typename GE>
 __device__ __forceinline__ uint64_t dcf_eval_g1(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
                                                 uint32_t party, uint32_t n, uint32_t bo, uint64_t x)
 {
-    const int ges = (int)((bo + 7) / 8);
-    uint32_t  s[4];
-    load_block_be(seed, s);
-    s[0] &= ~kSeedTBit;
-    uint32_t t   = party;
-    uint64_t acc = 0;
-#pragma unroll 1
-    for (uint32_t lv = 0; lv < n; lv++)
-    {
-        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
-        const uint64_t vcw = (uint64_t)__ldg(K.vCW + lv);
-        uint32_t       v[4];
-        const uint32_t tp = t;
-        t                 = dcf_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv, v);
-        const uint64_t val = block_le_prefix(v, ges) + (tp ? vcw : 0);
-        acc += party ? (0 - val) : val;
-    }
-    const uint64_t val = block_le_prefix(s, ges) + (t ? (uint64_t)__ldg(K.last) : 0);
-    acc += party ? (0 - val) : val;
-    return acc;
+    const uint64_t xs[1] = {x};
+    uint64_t       acc[1];
+    if (sizeof(GE) <= 4 || bo <= 32)
+        dcf_eval_g1_vw<GE, 1, 1>(A, K, seed, party, n, bo, xs, acc);
+    else
+        dcf_eval_g1_vw<GE, 1, 2>(A, K, seed, party, n, bo, xs, acc);
+    return acc[0];
+}
+
+// Shares at two points under one key, both walks in the same AES calls.
+template <typename GE>
+__device__ __forceinline__ void dcf_eval_g1_two(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
+                                                uint32_t party, uint32_t n, uint32_t bo, uint64_t xa, uint64_t xb,
+                                                uint64_t &sa, uint64_t &sb)
+{
+    const uint64_t xs[2] = {xa, xb};
+    uint64_t       acc[2];
+    if (sizeof(GE) <= 4 || bo <= 32)
+        dcf_eval_g1_vw<GE, 2, 1>(A, K, seed, party, n, bo, xs, acc);
+    else
+        dcf_eval_g1_vw<GE, 2, 2>(A, K, seed, party, n, bo, xs, acc);
+    sa = acc[0];
+    sb = acc[1];
 }
 
 // Key generation of one element (src/impl/dcf.h:187-368). beta == nullptr means beta = 1

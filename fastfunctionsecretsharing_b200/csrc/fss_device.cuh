@@ -190,6 +190,58 @@ __device__ __forceinline__ void aes_encrypt(const AesLanes& A, const uint32_t ke
     for (int b = 0; b < NB; b++) enc_last(A, st[b], w);
 }
 
+// Blocks 2 dir and 2 dir + 1 of the GGM expansion under `key`: the seed child (all four words,
+// into sOut) and the value child (its first VW words, into vOut). Their plaintexts differ only
+// in bytes 0 and 8, which feed one lookup each of first-round columns 0 and 2, so the other 14
+// first-round lookups are shared; the value child's last round computes only the VW columns
+// that are read. Lookups: 40 (schedule) + 160 (seed child) + 160 - 14 - 4 (4 - VW) (value).
+// NK independent nodes (keys and directions) are expanded side by side, round by round.
+template <int NK, int VW>
+__device__ __forceinline__ void aes_prg_pair(const AesLanes& A, const uint32_t key[NK][4], const uint32_t dir[NK],
+                                             uint32_t sOut[NK][4], uint32_t vOut[NK][VW])
+{
+    uint32_t w[NK][4], sa[NK][4], sb[NK][4];
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) w[k][c] = key[k][c];
+        const uint32_t a0 = w[k][0] ^ ((4u * dir[k]) << 24), b0 = w[k][0] ^ ((4u * dir[k] + 2u) << 24);
+        const uint32_t a2 = w[k][2] ^ ((4u * dir[k] + 1u) << 24), b2 = w[k][2] ^ ((4u * dir[k] + 3u) << 24);
+        const uint32_t s1 = w[k][1], s3 = w[k][3];
+        key_step(A, w[k], 0x01u);
+        // round 1: bytes other than the MSBs of words 0 and 2 are the same in both states
+        const uint32_t x0 = te<1, 2>(A, s1) ^ te<2, 1>(A, a2) ^ te<3, 0>(A, s3) ^ w[k][0];
+        const uint32_t t1 = te<0, 3>(A, s1) ^ te<1, 2>(A, a2) ^ te<2, 1>(A, s3) ^ te<3, 0>(A, a0) ^ w[k][1];
+        const uint32_t x2 = te<1, 2>(A, s3) ^ te<2, 1>(A, a0) ^ te<3, 0>(A, s1) ^ w[k][2];
+        const uint32_t t3 = te<0, 3>(A, s3) ^ te<1, 2>(A, a0) ^ te<2, 1>(A, s1) ^ te<3, 0>(A, a2) ^ w[k][3];
+        sa[k][0] = te<0, 3>(A, a0) ^ x0, sa[k][1] = t1, sa[k][2] = te<0, 3>(A, a2) ^ x2, sa[k][3] = t3;
+        sb[k][0] = te<0, 3>(A, b0) ^ x0, sb[k][1] = t1, sb[k][2] = te<0, 3>(A, b2) ^ x2, sb[k][3] = t3;
+    }
+    constexpr uint32_t RCON[10] = {0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80, 0x1b, 0x36};
+#pragma unroll
+    for (int r = 1; r < 9; r++)
+    {
+#pragma unroll
+        for (int k = 0; k < NK; k++)
+        {
+            key_step(A, w[k], RCON[r]);
+            enc_round(A, sa[k], w[k]);
+            enc_round(A, sb[k], w[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NK; k++)
+    {
+        key_step(A, w[k], RCON[9]);
+        enc_last(A, sa[k], w[k]);
+#pragma unroll
+        for (int c = 0; c < 4; c++) sOut[k][c] = sa[k][c];
+        vOut[k][0] = sub_col(A, sb[k][0], sb[k][1], sb[k][2], sb[k][3]) ^ w[k][0];
+        if (VW > 1) vOut[k][VW > 1 ? 1 : 0] = sub_col(A, sb[k][1], sb[k][2], sb[k][3], sb[k][0]) ^ w[k][1];
+    }
+}
+
 // NK independent keys, NB blocks under each. The round loop is not unrolled (small code for
 // the kernels that instantiate several of these); inside an iteration the block rounds under
 // round key r and the schedule step to round key r + 1 are independent, so they overlap.

@@ -22,8 +22,8 @@ __device__ __forceinline__ GE mic_eval_item(const AesLanes &A, const GE *maskedX
     const uint64_t xP = mod_bits<GE>((uint64_t)(GE)(x - 1 - L), n);
     const uint64_t xQ = mod_bits<GE>((uint64_t)(GE)(x - 1 - qP), n);
     const uint64_t p  = mod_bits<GE>(L, n);
-    const uint64_t sp = dcf_eval_g1<GE>(A, K, seed + 16 * i, party, n, bo, xP);
-    const uint64_t sq = dcf_eval_g1<GE>(A, K, seed + 16 * i, party, n, bo, xQ);
+    uint64_t       sp, sq;
+    dcf_eval_g1_two<GE>(A, K, seed + 16 * i, party, n, bo, xP, xQ, sp, sq);
     uint64_t       o  = sq - sp + (uint64_t)__ldg(z + w);
     if (party == 1) o += (uint64_t)((int64_t)(x > p) - (int64_t)(x > qP));
     return (GE)o;

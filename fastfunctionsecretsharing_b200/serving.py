@@ -8,15 +8,20 @@ as a Poisson process. The server
 * keeps key material device-resident in a key store whose capacity is counted in bytes; a
   request is admitted only when its keys fit in the remaining capacity (charged on
   admission, released on completion);
-* batches continuously: whatever has been admitted since the last launch goes out as one
-  persistent batched launch on a free stream slot while earlier batches are still running on
-  the other slots (up to `slots` launches in flight); a request's masked input is copied in
-  from pinned host memory and its shares copied back on the same stream;
+* batches continuously: admitted requests are taken from the head of the FIFO queue into one
+  persistent batched launch until the batch's estimated GPU time (algorithmic AES lookups at
+  the lookup rate of the kernels) reaches `batch_cap_ms`, so early arrivals are not held back
+  behind everything queued after them; a new batch goes out on a free stream slot while at
+  most `max_inflight - 1` earlier batches are still queued or running, so the device never
+  idles between batches and a request waits behind a bounded amount of work. A request's
+  masked input is copied in from pinned host memory and its shares copied back on the same
+  stream;
 * records per-request latency (completion - arrival, wall clock; completion is observed by
   polling the launch's CUDA event).
 
 The `plain` mode serves the same arrivals without batching: every admitted request is its own
-per-call C-ABI evaluation, queued FIFO on one stream.
+per-call C-ABI evaluation, queued FIFO on one stream (the spline cache the per-call API
+requires is allocated once per size class, not per call).
 
 Key material: the store charges every request its key bytes; the kernels read valid keys from
 one pool per kind and size class, so every evaluation is real and checkable while the 64 GB
@@ -35,7 +40,7 @@ import torch
 
 from . import _lib, batch
 from . import dcf_key_gen, spline_get_cache_data_size, spline_key_gen
-from .workloads import _rand_ring, _ring_tensor, partition
+from .workloads import _rand_ring, _ring_tensor, algorithmic_lookups, dcf_level_lookups, partition
 
 DCF_N = 32
 SPLINE_N, SPLINE_M, SPLINE_D = 64, 32, 2
@@ -67,6 +72,7 @@ class SizeClass:
     seed: torch.Tensor
     e: torch.Tensor | None = None
     beta: torch.Tensor | None = None
+    cache: torch.Tensor | None = None  # the spline eval cache the per-call API requires (reused)
 
 
 @dataclass
@@ -109,7 +115,9 @@ def make_pools(device, dcf_log2=(10, 20), spline_log2=(10, 14), seed=9, party=0)
         e0, b0 = _rand_ring(gen, e.shape, 8, dev), _rand_ring(gen, beta.shape, 8, dev)
         if party == 1:
             e0, b0 = e - e0, beta - b0
-        P.spline[N] = SizeClass(N, key, s0 if party == 0 else s1, e0, b0)
+        cache = torch.empty(spline_get_cache_data_size(SPLINE_D, SPLINE_M, SPLINE_N, SPLINE_N, 8, N),
+                            dtype=torch.uint8, device=dev)
+        P.spline[N] = SizeClass(N, key, s0 if party == 0 else s1, e0, b0, cache)
     torch.cuda.synchronize(dev)
     return P
 
@@ -176,14 +184,44 @@ def make_requests(P: Pools, rate: float, count: int, seed: int = 1, dcf_log2=(10
     return out
 
 
+# Estimated evaluation cost (AES table lookups) per element, used to cap a batch's GPU time.
+DCF_LOOKUPS = DCF_N * dcf_level_lookups(DCF_N)
+SPLINE_LOOKUPS = algorithmic_lookups("spline", 1, SPLINE_N, SPLINE_N, SPLINE_M, SPLINE_D)
+
+
+def request_lookups(r: Request) -> int:
+    return r.size * (DCF_LOOKUPS if r.kind == "dcf" else SPLINE_LOOKUPS)
+
+
 class Server:
-    def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=4, tuning: batch.Tuning | None = None):
+    def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=4, tuning: batch.Tuning | None = None,
+                 max_inflight: int = 2, batch_cap_ms: float = 4.0, lookups_per_s: float = 8.0e12):
         self.P = pools
         self.dev = pools.dev
         self.store = KeyStore(capacity_bytes)
         self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
-        self.tuning = tuning or batch.Tuning(256, 1 << 26, 0, 0)
+        self.tuning = tuning or batch.Tuning(512, 1 << 26, 0, 0)
+        self.max_inflight = max(1, min(max_inflight, slots))
+        self.batch_cap = batch_cap_ms * 1e-3 * lookups_per_s
         self.launches = 0
+        self.batch_log: list | None = None  # set to [] to record per-batch host time and kernel events
+
+    def warmup(self) -> None:
+        """One request of every size class through both paths, synchronously: loads the kernels
+        and fills the allocator's caches before anything is timed."""
+        reqs = []
+        for kind, pool in (("dcf", self.P.dcf), ("spline", self.P.spline)):
+            for n in pool:
+                dt = torch.int32 if kind == "dcf" else torch.int64
+                reqs.append(Request(-1, kind, 0, n, 0.0, 0, x_host=torch.zeros(n, dtype=dt).pin_memory(),
+                                    out_host=torch.empty(n, dtype=dt).pin_memory()))
+        s = self.slots[0]
+        with torch.cuda.stream(s):
+            for r in reqs:
+                self._plain_call(r, s)
+            built = [self._build(r) for r in reqs]
+            batch.Batch(built, self.dev).prepare(self.tuning).launch()
+        torch.cuda.synchronize(self.dev)
 
     def _build(self, r: Request) -> batch.Request:
         """Device buffers and the batch request of r (input copied in on the current stream)."""
@@ -220,8 +258,8 @@ class Server:
             x = torch.empty(r.size, dtype=torch.int64, device=self.dev)
             x.copy_(r.x_host, non_blocking=True)
             out = torch.empty(r.size, dtype=torch.int64, device=self.dev)
-            csize = spline_get_cache_data_size(SPLINE_D, SPLINE_M, SPLINE_N, SPLINE_N, 8, r.size)
-            cache = torch.empty(csize, dtype=torch.uint8, device=self.dev)
+            cache = c.cache
+            csize = cache.numel()
             rc = _lib.fn("FastFss_cuda_dcfSplineEval")(
                 out.data_ptr(), 8 * r.size, x.data_ptr(), 8 * r.size, c.key.data_ptr(), c.key.numel(),
                 c.e.data_ptr(), 8 * g * r.size, c.beta.data_ptr(), 8 * g * r.size, c.seed.data_ptr(), 16 * r.size,
@@ -259,17 +297,29 @@ class Server:
                     still.append((ev, si, rs, keep))
             inflight = still
             if mode == "batched":
-                if pending and free:
-                    admitted = []
-                    while pending and self.store.try_admit(pending[0].key_bytes):
+                if pending and free and len(inflight) < self.max_inflight:
+                    admitted, cost = [], 0
+                    while pending and (not admitted or cost + request_lookups(pending[0]) <= self.batch_cap) \
+                            and self.store.try_admit(pending[0].key_bytes):
+                        cost += request_lookups(pending[0])
                         admitted.append(pending.popleft())
                     if admitted:
                         si = free.pop()
                         s = self.slots[si]
+                        h0 = time.perf_counter()
                         with torch.cuda.stream(s):
                             reqs = [self._build(r) for r in admitted]
                             b = batch.Batch(reqs, self.dev).prepare(self.tuning)
+                            if self.batch_log is not None:
+                                e0 = torch.cuda.Event(enable_timing=True)
+                                e0.record(s)
                             b.launch()
+                            if self.batch_log is not None:
+                                e1 = torch.cuda.Event(enable_timing=True)
+                                e1.record(s)
+                                self.batch_log.append({"requests": len(admitted), "lookups": cost,
+                                                       "host_ms": (time.perf_counter() - h0) * 1e3,
+                                                       "events": (e0, e1)})
                             for r, q in zip(admitted, reqs):
                                 r.out_host.copy_(q.tensors[0].view(-1), non_blocking=True)
                             ev = torch.cuda.Event()

@@ -75,6 +75,46 @@ def _ring_tensor(vals, es, dev):
     return torch.from_numpy(arr.view({1: np.int8, 2: np.int16, 4: np.int32, 8: np.int64}[es]).copy()).to(dev)
 
 
+def dcf_level_lookups(bo: int) -> int:
+    """AES table lookups of one groupSize-1 DCF level: key schedule (40), the seed child (160) and
+    the value child less the 14 first-round lookups it shares with the seed child and the
+    last-round columns a ceil(bo/8)-byte read does not need (4 per unused column)."""
+    cols = 1 if (bo + 7) // 8 <= 4 else 2
+    return 40 + 160 + 160 - 14 - 4 * (4 - cols)
+
+
+def spline_window_blocks(m: int, cn: int, c0: int, cnt: int, ges: int) -> int:
+    """Convert-stream blocks read per level for coefficients c0 .. c0 + cnt - 1 of an interval
+    (the maximum over the intervals' byte offsets, as the kernels use it)."""
+    nb = 1
+    for q in range(min(m, 16)):
+        off = ((q * cn + c0) * ges) & 15
+        nb = max(nb, (off + cnt * ges + 15) >> 4)
+    return nb
+
+
+def algorithmic_lookups(kind: str, N: int, n: int, bo: int, m: int = 0, d: int = 0) -> int:
+    """AES table lookups one party's evaluation needs.
+
+    mic: 2 m groupSize-1 DCF walks of n levels per element.
+    spline: per element and interval, two DCF walks of n levels; a level is the node expansion
+    (key schedule + seed child + full value child, 346) and the convert of interval q's d + 1
+    values out of the value child's AES-CTR stream (key schedule + the blocks holding them);
+    the leaf adds one more convert per walk. Values are read 4 at a time."""
+    if kind == "mic":
+        return N * m * 2 * n * dcf_level_lookups(bo)
+    if kind == "spline":
+        cn, ges = d + 1, (bo + 7) // 8
+        g = m * cn
+        conv = 0
+        for c0 in range(0, cn, 4):
+            cnt = min(4, cn - c0)
+            conv += (40 + 160 * spline_window_blocks(m, cn, c0, cnt, ges)) if ges * g > 16 else 0
+        steps = 1 + (cn - 1) // 4  # the walks are repeated per pass of 4 coefficients
+        return N * m * 2 * (steps * n * 346 + (n + 1) * conv)
+    raise ValueError(kind)
+
+
 @dataclass
 class Instance:
     kind: str
@@ -85,6 +125,7 @@ class Instance:
     plain: tuple  # (ctypes function, argument tuple) of the per-call C ABI evaluation
     out_plain: torch.Tensor
     key_bytes: int
+    lookups: int = 0  # algorithmic AES table lookups of one evaluation
 
 
 def _stream_arg(dev):
@@ -132,7 +173,8 @@ def mixed_mic_spline(device="cuda", instances=256, seed=4, mic_log2=(8, 18), spl
                     zs.data_ptr(), zs.numel() * es, seed_p.data_ptr(), N * 16, party, Lt.data_ptr(), Lt.numel() * es,
                     Rt.data_ptr(), Rt.numel() * es, n, bo, es, N, None, 0, ctypes.byref(stream_h))
             req.tensors += [o_p]
-            out.append(Instance("mic", n, es, N, req, (fn, args), o_p, key.numel()))
+            out.append(Instance("mic", n, es, N, req, (fn, args), o_p, key.numel(),
+                                algorithmic_lookups("mic", N, n, bo, mic_intervals)))
         else:
             m, d = spline_intervals, degree
             L, R = partition(rng, m, n)
@@ -158,7 +200,8 @@ def mixed_mic_spline(device="cuda", instances=256, seed=4, mic_log2=(8, 18), spl
                     m * es, Rt.data_ptr(), m * es, m, d, n, bo, es, N, cache.data_ptr(), csize,
                     ctypes.byref(stream_h))
             req.tensors += [o_p, cache]
-            out.append(Instance("spline", n, es, N, req, (fn, args), o_p, key.numel()))
+            out.append(Instance("spline", n, es, N, req, (fn, args), o_p, key.numel(),
+                                algorithmic_lookups("spline", N, n, bo, m, d)))
         del s0, s1
     torch.cuda.synchronize(dev)
     return out
