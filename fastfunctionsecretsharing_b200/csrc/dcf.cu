@@ -155,7 +155,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfKeyGen(void *key, size_t keyDataSize
         cudaStream_t stream = resolve_stream(cudaStreamPtr);
         auto         kern   = dcf_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N, kDcfThreads, 1), kDcfThreads, kAesSmemTotal, stream>>>(
+        kern<<<grid_for(N, aes_threads(N, kDcfThreads), 1), aes_threads(N, kDcfThreads), kAesSmemTotal, stream>>>(
             (uint8_t *)key, (const GE *)alpha, (const GE *)beta, (const uint8_t *)seed0, (const uint8_t *)seed1,
             (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, (uint32_t)groupSize, N);
         return launch_status();
@@ -190,7 +190,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfEval(void *sharedOut, size_t sharedO
         {
             auto kern = dcf_eval_g1_kernel<GE>;
             if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-            kern<<<grid_for(N, kDcfThreads, 1), kDcfThreads, kAesSmemTotal, stream>>>(
+            kern<<<grid_for(N, aes_threads(N, kDcfThreads), 1), aes_threads(N, kDcfThreads), kAesSmemTotal, stream>>>(
                 (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                 (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, N);
         }
@@ -198,7 +198,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfEval(void *sharedOut, size_t sharedO
         {
             auto kern = dcf_eval_kernel<GE>;
             if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-            kern<<<grid_for(N, kDcfThreads, 1), kDcfThreads, kAesSmemTotal, stream>>>(
+            kern<<<grid_for(N, aes_threads(N, kDcfThreads), 1), aes_threads(N, kDcfThreads), kAesSmemTotal, stream>>>(
                 (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                 (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, (uint32_t)groupSize, N);
         }

@@ -151,7 +151,7 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
     cudaStream_t stream = resolve_stream(cudaStreamPtr);
     auto         kern   = dpf_eval_kernel<GE, MODE>;
     if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-    kern<<<grid_for(work, kDpfThreads, 1), kDpfThreads, kAesSmemTotal, stream>>>(
+    kern<<<grid_for(work, aes_threads(work, kDpfThreads), 1), aes_threads(work, kDpfThreads), kAesSmemTotal, stream>>>(
         (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (const GE *)point,
         (uint32_t)partyId, (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, per, work);
     return launch_status();
@@ -190,7 +190,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dpfKeyGen(void *key, size_t keyDataSize
         cudaStream_t stream = resolve_stream(cudaStreamPtr);
         auto         kern   = dpf_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N, kDpfThreads, 1), kDpfThreads, kAesSmemTotal, stream>>>(
+        kern<<<grid_for(N, aes_threads(N, kDpfThreads), 1), aes_threads(N, kDpfThreads), kAesSmemTotal, stream>>>(
             (uint8_t *)key, (const GE *)alpha, (const GE *)beta, (const uint8_t *)seed0, (const uint8_t *)seed1,
             (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, (uint32_t)groupSize, N);
         return launch_status();

@@ -86,6 +86,23 @@ inline unsigned grid_for(std::size_t work, int threads, int perSm)
     return (unsigned)need;
 }
 
+// CTA size for an AES kernel (one CTA per SM, `maxThreads` threads at most) over `work` items
+// taken grid-stride: the smallest whole number of warps that still covers the work in the
+// same number of passes k = ceil(work / (SMs * maxThreads)), so that the last pass is not a
+// partial wave on a few SMs and a small launch runs on every SM instead of a few full ones
+// (at least 64 threads).
+inline int aes_threads(std::size_t work, int maxThreads)
+{
+    const std::size_t sms   = (std::size_t)sm_count();
+    const std::size_t full  = sms * (std::size_t)maxThreads;
+    const std::size_t k     = work == 0 ? 1 : (work + full - 1) / full;
+    std::size_t       t     = (work + sms * k - 1) / (sms * k);
+    t                       = ((t + 31) / 32) * 32;
+    if (t < 64) t = 64;
+    if (t > (std::size_t)maxThreads) t = (std::size_t)maxThreads;
+    return (int)t;
+}
+
 // Every AES kernel takes the replicated T-tables (kAesSmemTotal bytes of dynamic shared
 // memory, declared in fss_device.cuh).
 template <typename K>

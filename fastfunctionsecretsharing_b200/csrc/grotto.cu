@@ -375,7 +375,8 @@ template <typename K, typename... Args>
 static int launch(K kern, size_t work, cudaStream_t stream, Args... args)
 {
     if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-    kern<<<grid_for(work, kGrottoThreads, 1), kGrottoThreads, kAesSmemTotal, stream>>>(args...);
+    const int threads = aes_threads(work, kGrottoThreads);
+    kern<<<grid_for(work, threads, 1), threads, kAesSmemTotal, stream>>>(args...);
     return launch_status();
 }
 

@@ -98,7 +98,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfMICKeyGen(void *key, size_t keyDataS
         if (N == 0) return FAST_FSS_SUCCESS;
         auto kern = mic_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N, kMicThreads, 1), kMicThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
+        kern<<<grid_for(N, aes_threads(N, kMicThreads), 1), aes_threads(N, kMicThreads), kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
             (uint8_t *)key, (GE *)z, (const GE *)alpha, (const uint8_t *)seed0, (const uint8_t *)seed1,
             (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)bitWidthIn,
             (uint32_t)bitWidthOut, N);
@@ -134,7 +134,8 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfMICEval(void *sharedOut, size_t shar
         if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
         auto kern = mic_eval_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N * m, kMicThreads, 1), kMicThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
+        kern<<<grid_for(N * m, aes_threads(N * m, kMicThreads), 1), aes_threads(N * m, kMicThreads), kAesSmemTotal,
+                 resolve_stream(cudaStreamPtr)>>>(
             (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const GE *)sharedZ, (const uint8_t *)seed,
             (uint32_t)partyId, (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)n,
             (uint32_t)bitWidthOut, N);

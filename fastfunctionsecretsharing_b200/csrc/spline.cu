@@ -133,7 +133,8 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfSplineKeyGen(
         if (N == 0) return FAST_FSS_SUCCESS;
         auto kern = spline_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N, kSplineThreads, 1), kSplineThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
+        kern<<<grid_for(N, aes_threads(N, kSplineThreads), 1), aes_threads(N, kSplineThreads), kAesSmemTotal,
+                 resolve_stream(cudaStreamPtr)>>>(
             (uint8_t *)key, (GE *)e, (GE *)beta, (const GE *)alpha, (const uint8_t *)seed0, (const uint8_t *)seed1,
             (const GE *)coefficients, (uint32_t)degree, (const GE *)leftEndpoints, (const GE *)rightEndpoints,
             (uint32_t)m, (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, N);
@@ -173,7 +174,8 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfSplineEval(
         while (G < 32 && G < m) G <<= 1;
         auto kern = spline_eval_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N * G, kSplineEvalThreads, 1), kSplineEvalThreads, kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
+        kern<<<grid_for(N * G, aes_threads(N * G, kSplineEvalThreads), 1), aes_threads(N * G, kSplineEvalThreads),
+                 kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
             (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const GE *)sharedE, (const GE *)sharedBeta,
             (const uint8_t *)seed, (uint32_t)partyId, (const GE *)leftEndpoints, (const GE *)rightEndpoints,
             (uint32_t)m, (uint32_t)degree, (uint32_t)bitWidthIn, (uint32_t)bitWidthOut, N, G);
