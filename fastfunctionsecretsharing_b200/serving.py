@@ -31,6 +31,7 @@ model stays within one GPU.
 from __future__ import annotations
 
 import ctypes
+import gc
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -272,7 +273,18 @@ class Server:
         return keep
 
     def run(self, requests: list[Request], mode: str = "batched", poll_s: float = 2e-5) -> float:
-        """Serves `requests` in real time; returns the makespan in seconds."""
+        """Serves `requests` in real time; returns the makespan in seconds. Python's cyclic
+        garbage collector is paused meanwhile (a full collection over the pools' and requests'
+        objects would stall the loop for tens of milliseconds)."""
+        was = gc.isenabled()
+        gc.disable()
+        try:
+            return self._run(requests, mode, poll_s)
+        finally:
+            if was:
+                gc.enable()
+
+    def _run(self, requests: list[Request], mode: str, poll_s: float) -> float:
         pending: deque[Request] = deque()
         arrivals = deque(sorted(requests, key=lambda r: r.arrival))
         inflight = []  # (event, slot index or None, [requests], keep-alive)
