@@ -24,7 +24,7 @@
 namespace fss {
 
 constexpr int kSplineThreads     = 256; // key generation
-constexpr int kSplineEvalThreads = 512; // evaluation: 16 warps per SM at <= 128 registers
+constexpr int kSplineEvalThreads = 256; // evaluation: 8 warps per SM, registers unconstrained
 
 // splineShiftPolynomialCoefficients (src/impl/spline.h:89-117), writing d + 1 values.
 template <typename GE>
