@@ -91,6 +91,7 @@ SIGNATURES: dict[str, tuple] = {
 EXTENSION_SIGNATURES: dict[str, tuple] = {
     "FastFss_b200_smemLookupProbe": (_I, [_P, _S, ctypes.c_uint, _P, _P]),
     "FastFss_b200_smCount": (_I, []),
+    "FastFss_b200_stageTimeouts": (_I, [_P]),
     "FastFss_cuda_grottoEqEvalAll": (_I, [_P, _S, _P, _S, _P, _S, _I, _S, _S, _S, _P]),
     "FastFss_cuda_grottoLeEvalAll": (_I, [_P, _S, _P, _S, _P, _S, _I, _S, _S, _S, _P]),
     "FastFss_cuda_grottoIntervalLutEvalFromRows": (

@@ -174,6 +174,10 @@ static int validate(const FastFssBatchOp &o)
         return FAST_FSS_RUNTIME_ERROR;
     if (o.kind == FAST_FSS_BATCH_SPLINE_EVAL && (!o.aux0 || !o.aux1 || !o.leftEndpoints || !o.rightEndpoints))
         return FAST_FSS_RUNTIME_ERROR;
+    if (int rc = check_alignment(es, {o.sharedOut, o.maskedX, o.aux0, o.aux1, o.leftEndpoints, o.rightEndpoints},
+                                 {o.key, o.seed});
+        rc != FAST_FSS_SUCCESS)
+        return rc;
     return FAST_FSS_SUCCESS;
 }
 

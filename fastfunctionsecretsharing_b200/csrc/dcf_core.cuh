@@ -100,13 +100,12 @@ __device__ __forceinline__ void dcf_eval_slice(const AesLanes &A, uint64_t out[M
 // One level for groupSize 1 of NK walks under the same key (correction words shared): like
 // dcf_step, but each value child is produced only as far as its first VW words (the bytes a
 // groupSize-1 convert reads: ceil(bo / 8) <= 4 VW).
+// The correction word cw[] (big-endian words) is supplied by the caller.
 template <int NK, int VW>
-__device__ __forceinline__ void dcf_step_g1(const AesLanes &A, uint32_t s[NK][4], uint32_t t[NK],
-                                            const uint32_t dir[NK], const uint8_t *cwp, uint64_t tl, uint64_t tr,
-                                            uint32_t lv, uint32_t v[NK][VW])
+__device__ __forceinline__ void dcf_step_g1_cw(const AesLanes &A, uint32_t s[NK][4], uint32_t t[NK],
+                                               const uint32_t dir[NK], const uint32_t cw[4], uint64_t tl, uint64_t tr,
+                                               uint32_t lv, uint32_t v[NK][VW])
 {
-    uint32_t cw[4];
-    load_block_be(cwp, cw);
     uint32_t sn[NK][4];
     aes_prg_pair<NK, VW>(A, s, dir, sn, v);
 #pragma unroll
@@ -120,6 +119,16 @@ __device__ __forceinline__ void dcf_step_g1(const AesLanes &A, uint32_t s[NK][4]
         tn ^= (uint32_t)(((dir[k] ? tr : tl) >> lv) & 1u) & t[k];
         t[k] = tn;
     }
+}
+
+template <int NK, int VW>
+__device__ __forceinline__ void dcf_step_g1(const AesLanes &A, uint32_t s[NK][4], uint32_t t[NK],
+                                            const uint32_t dir[NK], const uint8_t *cwp, uint64_t tl, uint64_t tr,
+                                            uint32_t lv, uint32_t v[NK][VW])
+{
+    uint32_t cw[4];
+    load_block_be(cwp, cw);
+    dcf_step_g1_cw<NK, VW>(A, s, t, dir, cw, tl, tr, lv, v);
 }
 
 // Little-endian value of the first `nbytes` (1 .. 4 VW) bytes of a block's first VW words.

@@ -148,6 +148,7 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
 {
     const size_t work = (MODE == 0) ? N : N * per;
     if (work == 0) return FAST_FSS_SUCCESS;
+    if (int rc = check_alignment(sizeof(GE), {out, maskedX, point}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
     cudaStream_t stream = resolve_stream(cudaStreamPtr);
     auto         kern   = dpf_eval_kernel<GE, MODE>;
     if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
@@ -187,6 +188,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dpfKeyGen(void *key, size_t keyDataSize
         }
         if (seedDataSize0 != N * 16 || seedDataSize1 != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {alpha, beta}, {key, seed0, seed1}); rc != FAST_FSS_SUCCESS) return rc;
         cudaStream_t stream = resolve_stream(cudaStreamPtr);
         auto         kern   = dpf_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;

@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <initializer_list>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -109,6 +110,24 @@ template <typename K>
 inline bool prepare_aes_kernel(K kernel)
 {
     return ensure_smem(reinterpret_cast<const void *>(kernel), 2 * 65536 + 256);
+}
+
+// Kernels read keys and seeds as 16-byte vectors and ring elements at their natural width;
+// the reference requires 16-byte aligned keys (include/FastFss/cuda/dcf.h:25-26) and leaves
+// misaligned buffers undefined. Here they are refused before any launch.
+inline bool aligned_to(const void *p, std::size_t a)
+{
+    return ((std::uintptr_t)p & (a - 1)) == 0;
+}
+
+inline int check_alignment(std::size_t es, std::initializer_list<const void *> ring,
+                           std::initializer_list<const void *> blocks)
+{
+    for (const void *p : ring)
+        if (!aligned_to(p, es)) return FAST_FSS_RUNTIME_ERROR;
+    for (const void *p : blocks)
+        if (!aligned_to(p, 16)) return FAST_FSS_RUNTIME_ERROR;
+    return FAST_FSS_SUCCESS;
 }
 
 inline int launch_status()

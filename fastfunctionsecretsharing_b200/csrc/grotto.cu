@@ -398,6 +398,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoKeyGen(void *key, size_t keyDataS
         if (seedDataSize0 != N * 16 || seedDataSize1 != N * 16) return FAST_FSS_INVALID_SEED_DATA_SIZE_ERROR;
         if (keyDataSize != grotto_key_bytes(bitWidthIn, es, N)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {alpha}, {key, seed0, seed1}); rc != FAST_FSS_SUCCESS) return rc;
         return launch(grotto_keygen_kernel<GE>, N, resolve_stream(cudaStreamPtr), (uint8_t *)key, (const GE *)alpha,
                       (const uint8_t *)seed0, (const uint8_t *)seed1, (uint32_t)bitWidthIn, N);
     });
@@ -432,6 +433,8 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoEqEval(void *sharedBooleanOut, si
         int rc   = grotto_point_checks<GE>(sharedOutDataSize, maskedXDataSize, keyDataSize, seedDataSize, partyId,
                                          bitWidthIn, elementNum, cacheDataSize);
         if (rc != FAST_FSS_SUCCESS || elementNum == 0) return rc;
+        if (int ra = check_alignment(sizeof(GE), {sharedBooleanOut, maskedX}, {key, seed}); ra != FAST_FSS_SUCCESS)
+            return ra;
         return launch(grotto_eval_kernel<GE, 0>, elementNum, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
                       (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                       (uint32_t)bitWidthIn, false, elementNum);
@@ -451,6 +454,8 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoEval(void *sharedBooleanOut, size
         int rc   = grotto_point_checks<GE>(sharedOutDataSize, maskedXDataSize, keyDataSize, seedDataSize, partyId,
                                          bitWidthIn, elementNum, cacheDataSize);
         if (rc != FAST_FSS_SUCCESS || elementNum == 0) return rc;
+        if (int ra = check_alignment(sizeof(GE), {sharedBooleanOut, maskedX}, {key, seed}); ra != FAST_FSS_SUCCESS)
+            return ra;
         return launch(grotto_eval_kernel<GE, 1>, elementNum, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
                       (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                       (uint32_t)bitWidthIn, equalBound, elementNum);
@@ -483,6 +488,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoMICEval(void *sharedBooleanOut, s
         if (cacheDataSize != 0 && cacheDataSize != grotto_cache_bytes(n, N))
             return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedBooleanOut, maskedX, leftEndpoints, rightEndpoints}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         return launch(grotto_mic_kernel<GE>, N * m, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
                       (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                       (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)n, N);
@@ -518,6 +524,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoIntervalLutEval(
         if (cacheDataSize != 0 && cacheDataSize != grotto_cache_bytes(n, N))
             return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedOutE, sharedOutT, maskedX, leftEndpoints, rightEndpoints, lookUpTable}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         uint32_t G = 1;
         while (G < 32 && G < m) G <<= 1;
         cudaStream_t stream = resolve_stream(cudaStreamPtr);
@@ -549,6 +556,7 @@ static int grotto_all_entry(void *out, size_t outDataSize, const void *key, size
         if (outDataSize != N * (((size_t)1 << n) / 8)) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
         if (((uintptr_t)out & 7u) != 0) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         const uint32_t D = (uint32_t)n - 6;
         const uint32_t d = D < (uint32_t)kAllMaxSub ? D : (uint32_t)kAllMaxSub;
         return launch(grotto_all_kernel<GE, MODE>, N << (D - d), resolve_stream(cudaStreamPtr),
@@ -597,6 +605,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoIntervalLutEvalFromRows(
         if (partyId != 0 && partyId != 1) return FAST_FSS_INVALID_PARTY_ID_ERROR;
         if (leRowsDataSize != N * (((size_t)1 << n) / 8)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedOutE, sharedOutT, maskedX, leftEndpoints, rightEndpoints, lookUpTable}, {}); rc != FAST_FSS_SUCCESS) return rc;
         cudaStream_t  stream = resolve_stream(cudaStreamPtr);
         constexpr int LMAX   = 4;
         for (size_t j0 = 0; j0 < (lutNum ? lutNum : 1); j0 += LMAX)

@@ -96,6 +96,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfMICKeyGen(void *key, size_t keyDataS
         if (leftEndpointsDataSize != m * es || rightEndpointsDataSize != m * es)
             return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {z, alpha, leftEndpoints, rightEndpoints}, {key, seed0, seed1}); rc != FAST_FSS_SUCCESS) return rc;
         auto kern = mic_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
         kern<<<grid_for(N, aes_threads(N, kMicThreads), 1), aes_threads(N, kMicThreads), kAesSmemTotal, resolve_stream(cudaStreamPtr)>>>(
@@ -132,6 +133,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfMICEval(void *sharedOut, size_t shar
             return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
         if (cacheDataSize != 0 && cacheDataSize != N * 16 * n + N * es * n) return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedOut, maskedX, sharedZ, leftEndpoints, rightEndpoints}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         auto kern = mic_eval_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
         kern<<<grid_for(N * m, aes_threads(N * m, kMicThreads), 1), aes_threads(N * m, kMicThreads), kAesSmemTotal,

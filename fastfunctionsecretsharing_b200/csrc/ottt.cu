@@ -106,6 +106,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_otttKeyGen(void *key, size_t keyDataSiz
         if (n >= 64 || keyDataSize != N * (((size_t)1 << n) / 8)) return FAST_FSS_INVALID_KEY_DATA_SIZE_ERROR;
         if (alphaDataSize != N * es) return FAST_FSS_INVALID_ALPHA_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {alpha}, {}); rc != FAST_FSS_SUCCESS) return rc;
         ottt_keygen_kernel<GE><<<grid_for(N, 256, 8), 256, 0, resolve_stream(cudaStreamPtr)>>>(
             (uint8_t *)key, (const GE *)alpha, (uint32_t)n, N);
         return launch_status();
@@ -133,6 +134,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_otttLutEval(void *sharedOutE, size_t sh
         if (sharedOutTDataSize != N * es * lutNum) return FAST_FSS_INVALID_SHARED_OUT_DATA_SIZE_ERROR;
         if (maskedXDataSize != N * es) return FAST_FSS_INVALID_MASKED_X_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedOutE, sharedOutT, maskedX, lookUpTable}, {}); rc != FAST_FSS_SUCCESS) return rc;
         const size_t rowBytes = ((size_t)1 << n) / 8;
         const bool   words    = (rowBytes % 4 == 0) && (((uintptr_t)key & 3u) == 0);
         const size_t units    = words ? rowBytes / 4 : rowBytes;

@@ -131,6 +131,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfSplineKeyGen(
         if (rightEndpointsDataSize != m * es) return FAST_FSS_INVALID_BOUNDARY_DATA_SIZE_ERROR;
         if (coefficientsDataSize != m * (degree + 1) * es) return FAST_FSS_INVALID_BETA_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {e, beta, alpha, coefficients, leftEndpoints, rightEndpoints}, {key, seed0, seed1}); rc != FAST_FSS_SUCCESS) return rc;
         auto kern = spline_keygen_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
         kern<<<grid_for(N, aes_threads(N, kSplineThreads), 1), aes_threads(N, kSplineThreads), kAesSmemTotal,
@@ -170,6 +171,7 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfSplineEval(
         if (cache == nullptr || cacheDataSize != spline_cache_bytes(bitWidthIn, m, degree, es, N))
             return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
+        if (int rc = check_alignment(es, {sharedOut, maskedX, sharedE, sharedBeta, leftEndpoints, rightEndpoints}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         uint32_t G = 1;
         while (G < 32 && G < m) G <<= 1;
         auto kern = spline_eval_kernel<GE>;

@@ -23,6 +23,14 @@ FAST_FSS_API int FastFss_b200_smemLookupProbe(void *sink, size_t sinkBytes, unsi
 
 FAST_FSS_API int FastFss_b200_smCount(void);
 
+/* Number of staging failures since the library was loaded on the current device: a kernel's
+ * bounded wait for one of its own asynchronous shared-memory staging copies ran out, or a CTA
+ * found its shared-memory window unfit for aligned stages (the groupSize-1 DCF evaluation
+ * stages its correction words this way). Always 0 in normal operation; a nonzero count means
+ * some shares of that launch were not written. Synchronous: waits for the device's earlier
+ * work. */
+FAST_FSS_API int FastFss_b200_stageTimeouts(unsigned int *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -318,3 +318,28 @@ def test_unsupported_element_size(lib):
     for es in (3, 16):
         rc = lib.FastFss_cuda_dcfEval(None, 0, None, 0, None, 0, None, 0, 0, 8, 8, 1, es, 1, None, 0, None)
         assert rc == -11
+
+
+def test_misaligned_key_or_seed_is_refused(lib):
+    """Keys and seeds are read as 16-byte vectors: a key or seed pointer that is 8 but not 16
+    byte aligned is refused (FAST_FSS_RUNTIME_ERROR) after the reference's own checks pass and
+    before anything is launched (the pointers here are host addresses and are never read)."""
+    base = ctypes.addressof(BUF)
+    off = (8 - base) % 16  # base + off is 8 mod 16: aligned for every ring element, not for blocks
+    mis = ctypes.c_void_p(base + off)
+    for api, (spec, vals, _bad) in sorted(CASES.items()):
+        if api.startswith("ottt"):
+            continue  # OTTT keys are bit rows, read at byte/word granularity
+        args = []
+        for kind, name in spec:
+            v = vals[name]
+            if kind == "p":
+                args.append(mis)
+            elif kind == "i":
+                args.append(ctypes.c_int(v))
+            elif kind == "b":
+                args.append(ctypes.c_bool(v))
+            else:
+                args.append(sz(v))
+        args.append(None)
+        assert getattr(lib, f"FastFss_cuda_{api}")(*args) == -1, api

@@ -148,3 +148,34 @@ def test_full_size_reconstruction_dcf_n32(F):
     assert torch.equal((y0 + y1).view(-1), want)
     del key
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("es,n", [(4, 32), (8, 64), (2, 13), (1, 3)])
+def test_dcf_staged_eval_partial_tiles(F, oracle, es, n):
+    """groupSize-1 DCF evaluation stages correction words through shared memory, 32 elements
+    per warp and 4 levels per copy: element counts that leave partial warp tiles and widths
+    that leave a partial last copy give the oracle's shares, no staging wait runs out, and a
+    key that is not 16-byte aligned is refused before anything is launched."""
+    import ctypes
+
+    from fastfunctionsecretsharing_b200 import _lib
+
+    rng = np.random.default_rng(zlib.crc32(repr(("staged", es, n)).encode()))
+    for N in (1, 33, 4099):
+        a, b, s0 = rnd(rng, N, es, n), rnd(rng, N, es, 8 * es), seeds(rng, N)
+        s1 = seeds(rng, N)
+        kref = oracle.dcf_keygen(a, b, s0, s1, n, 8 * es, 1)
+        x = rnd(rng, N, es, 8 * es)
+        for p, s in ((0, s0), (1, s1)):
+            out = empty_ring(es)
+            F.dcf_eval(out, dev_ring(x), dev_bytes(kref), dev_bytes(s), p, n, 8 * es, 1)
+            assert np.array_equal(host(out, es), oracle.dcf_eval(x, kref, s, p, n, 8 * es, 1))
+    buf = torch.zeros(kref.size + 8, dtype=torch.uint8, device="cuda")
+    unaligned = buf[8:]
+    assert unaligned.data_ptr() % 16 == 8
+    with pytest.raises(RuntimeError, match="failed : -1"):
+        F.dcf_eval(empty_ring(es), dev_ring(x), unaligned, dev_bytes(s0), 0, n, 8 * es, 1)
+    torch.cuda.synchronize()
+    cnt = ctypes.c_uint(7)
+    assert _lib.fn("FastFss_b200_stageTimeouts")(ctypes.byref(cnt)) == 0
+    assert cnt.value == 0
