@@ -15,6 +15,8 @@
 #include "dpf_core.cuh"
 #include "fss_device.cuh"
 #include "fss_host.h"
+#include "region_a_map.h"
+#include "region_a_stage.cuh"
 
 namespace fss {
 
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     }
 }
 
-// mode 0: plain eval (work = N); mode 1: evalAll (work = N 2^n); mode 2: evalMulti (N P).
+// mode 1: evalAll (work = N 2^n); mode 2: evalMulti (N P). Plain eval is dpf_eval_staged_kernel.
 template <typename GE, int MODE>
 __global__ void __launch_bounds__(kDpfThreads, 1)
     dpf_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
@@ -132,6 +134,89 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     }
 }
 
+// Plain evaluation (mode 0) with region A staged per warp through shared memory
+// (region_a_stage.cuh; keys are 16-byte aligned, checked by the entry points). A warp whose
+// copy does not arrive in time counts the failure in g_dpf_stage_failures, drains and stops.
+__device__ unsigned int g_dpf_stage_failures;
+
+template <typename GE>
+__global__ void __launch_bounds__(kDpfThreads, 1)
+    dpf_eval_staged_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                           const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, uint32_t bo, uint32_t g,
+                           size_t N, const __grid_constant__ CUtensorMap sCWmap)
+{
+    if (!stage_window_ok())
+    {
+        if (threadIdx.x == 0) atomicAdd(&g_dpf_stage_failures, 1u);
+        return;
+    }
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const uint32_t lane = threadIdx.x & 31u, W = blockDim.x >> 5;
+    const size_t   tile0 = (size_t)blockIdx.x * W + (threadIdx.x >> 5), tstride = (size_t)gridDim.x * W;
+    const size_t   tiles = (N + 31) / 32;
+    const size_t   bstr  = sizeof(GE) * (2 + (size_t)g);
+    RegionAStage   S;
+    S.init(&sCWmap, n, N, tile0, tstride);
+    bool failed = false;
+    for (size_t T = tile0; T < tiles && !failed; T += tstride)
+    {
+        const size_t i      = T * 32 + lane;
+        const bool   active = i < N;
+        const GE    *kb     = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
+        uint64_t     x = 0, tl = 0, tr = 0;
+        uint32_t     s[4], t = party;
+        if (active)
+        {
+            x  = mod_bits<GE>((uint64_t)__ldg(maskedX + i), n);
+            tl = (uint64_t)__ldg(kb);
+            tr = (uint64_t)__ldg(kb + 1);
+            load_block_be(seed + 16 * i, s);
+            s[0] &= ~kSeedTBit;
+        }
+        for (uint32_t lv0 = 0; lv0 < n; lv0 += kStageLevels)
+        {
+            if (!S.wait())
+            {
+                failed = true;
+                break;
+            }
+            if (active)
+            {
+                const uint32_t lc = min((uint32_t)kStageLevels, n - lv0);
+#pragma unroll 1
+                for (uint32_t j = 0; j < lc; j++)
+                {
+                    const uint32_t lv = lv0 + j;
+                    uint32_t       cw[4];
+                    S.level(j, cw);
+                    t = dpf_step(A, s, t, (uint32_t)((x >> (n - 1 - lv)) & 1u), cw, tl, tr, lv);
+                }
+            }
+            S.next();
+        }
+        if (failed) break;
+        if (active) dpf_leaf<GE>(A, out + i * g, s, t, kb, party, bo, g);
+    }
+    if (failed)
+    {
+        if (lane == 0) atomicAdd(&g_dpf_stage_failures, 1u);
+        S.drain();
+    }
+}
+
+unsigned int dpf_stage_failures()
+{
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_dpf_stage_failures, sizeof(v)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 0xffffffffu;
+    }
+    return v;
+}
+
 static inline size_t dpf_key_bytes(size_t n, size_t g, size_t es, size_t N)
 {
     return N * (16 * n + es + es + es * g);
@@ -150,12 +235,29 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
     if (work == 0) return FAST_FSS_SUCCESS;
     if (int rc = check_alignment(sizeof(GE), {out, maskedX, point}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
     cudaStream_t stream = resolve_stream(cudaStreamPtr);
-    auto         kern   = dpf_eval_kernel<GE, MODE>;
-    if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-    kern<<<grid_for(work, aes_threads(work, kDpfThreads), 1), aes_threads(work, kDpfThreads), kAesSmemTotal, stream>>>(
-        (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (const GE *)point,
-        (uint32_t)partyId, (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, per, work);
-    return launch_status();
+    if constexpr (MODE == 0)
+    {
+        CUtensorMap map;
+        if (!encode_region_a_map(&map, key, n, N)) return FAST_FSS_RUNTIME_ERROR;
+        auto           kern    = dpf_eval_staged_kernel<GE>;
+        const int      threads = aes_threads(N, kDpfThreads);
+        if (!ensure_smem(reinterpret_cast<const void *>(kern), stage_smem_bytes(kDpfThreads / 32)))
+            return FAST_FSS_RUNTIME_ERROR;
+        kern<<<grid_for(N, threads, 1), threads, stage_smem_bytes(threads / 32), stream>>>(
+            (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+            (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, map);
+        return launch_status();
+    }
+    else
+    {
+        auto kern = dpf_eval_kernel<GE, MODE>;
+        if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
+        const int threads = aes_threads(work, kDpfThreads);
+        kern<<<grid_for(work, threads, 1), threads, kAesSmemTotal, stream>>>(
+            (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (const GE *)point,
+            (uint32_t)partyId, (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, per, work);
+        return launch_status();
+    }
 }
 
 } // namespace fss

@@ -74,15 +74,18 @@ def test_grid_vs_oracle(F, oracle, kind, es, n, bo, g):
 
 
 @pytest.mark.parametrize("N", [0, 1, 8, 1023, 1024, 2047, 2048])
-def test_element_counts(F, oracle, N):
+@pytest.mark.parametrize("kind", ["dcf", "dpf"])
+def test_element_counts(F, oracle, kind, N):
     rng = np.random.default_rng(N)
     es, n, bo, g = 4, 32, 32, 1
     a, b, s0, s1 = rnd(rng, N, es, n), rnd(rng, N, es, bo), seeds(rng, N), seeds(rng, N)
     x = rnd(rng, N, es, n)
-    key = _dcf(F, "dcf", a, b, s0, s1, n, bo, g)
-    assert np.array_equal(host(key), oracle.dcf_keygen(a, b, s0, s1, n, bo, g))
+    x[::7] = a[::7]
+    key = _dcf(F, kind, a, b, s0, s1, n, bo, g)
+    assert np.array_equal(host(key), getattr(oracle, f"{kind}_keygen")(a, b, s0, s1, n, bo, g))
     for p, s in ((0, s0), (1, s1)):
-        assert np.array_equal(_eval(F, "dcf", key, x, s, p, n, bo, g), oracle.dcf_eval(x, host(key), s, p, n, bo, g))
+        want = getattr(oracle, f"{kind}_eval")(x, host(key), s, p, n, bo, g)
+        assert np.array_equal(_eval(F, kind, key, x, s, p, n, bo, g), want)
 
 
 def test_beta_default_is_one(F, oracle):
@@ -151,11 +154,12 @@ def test_full_size_reconstruction_dcf_n32(F):
 
 
 @pytest.mark.parametrize("es,n", [(4, 32), (8, 64), (2, 13), (1, 3)])
-def test_dcf_staged_eval_partial_tiles(F, oracle, es, n):
-    """groupSize-1 DCF evaluation stages correction words through shared memory, 32 elements
-    per warp and 4 levels per copy: element counts that leave partial warp tiles and widths
-    that leave a partial last copy give the oracle's shares, no staging wait runs out, and a
-    key that is not 16-byte aligned is refused before anything is launched."""
+@pytest.mark.parametrize("kind", ["dcf", "dpf"])
+def test_staged_eval_partial_tiles(F, oracle, kind, es, n):
+    """groupSize-1 DCF and DPF evaluation stage correction words through shared memory, 32
+    elements per warp and 4 levels per copy: element counts that leave partial warp tiles and
+    widths that leave a partial last copy give the oracle's shares, no staging wait runs out,
+    and a key that is not 16-byte aligned is refused before anything is launched."""
     import ctypes
 
     from fastfunctionsecretsharing_b200 import _lib
@@ -164,17 +168,18 @@ def test_dcf_staged_eval_partial_tiles(F, oracle, es, n):
     for N in (1, 33, 4099):
         a, b, s0 = rnd(rng, N, es, n), rnd(rng, N, es, 8 * es), seeds(rng, N)
         s1 = seeds(rng, N)
-        kref = oracle.dcf_keygen(a, b, s0, s1, n, 8 * es, 1)
+        kref = getattr(oracle, f"{kind}_keygen")(a, b, s0, s1, n, 8 * es, 1)
         x = rnd(rng, N, es, 8 * es)
+        x[::3] = a[::3]
         for p, s in ((0, s0), (1, s1)):
             out = empty_ring(es)
-            F.dcf_eval(out, dev_ring(x), dev_bytes(kref), dev_bytes(s), p, n, 8 * es, 1)
-            assert np.array_equal(host(out, es), oracle.dcf_eval(x, kref, s, p, n, 8 * es, 1))
+            getattr(F, f"{kind}_eval")(out, dev_ring(x), dev_bytes(kref), dev_bytes(s), p, n, 8 * es, 1)
+            assert np.array_equal(host(out, es), getattr(oracle, f"{kind}_eval")(x, kref, s, p, n, 8 * es, 1))
     buf = torch.zeros(kref.size + 8, dtype=torch.uint8, device="cuda")
     unaligned = buf[8:]
     assert unaligned.data_ptr() % 16 == 8
     with pytest.raises(RuntimeError, match="failed : -1"):
-        F.dcf_eval(empty_ring(es), dev_ring(x), unaligned, dev_bytes(s0), 0, n, 8 * es, 1)
+        getattr(F, f"{kind}_eval")(empty_ring(es), dev_ring(x), unaligned, dev_bytes(s0), 0, n, 8 * es, 1)
     torch.cuda.synchronize()
     cnt = ctypes.c_uint(7)
     assert _lib.fn("FastFss_b200_stageTimeouts")(ctypes.byref(cnt)) == 0
