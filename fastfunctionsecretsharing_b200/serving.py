@@ -11,9 +11,14 @@ as a Poisson process. The server
 * batches continuously: admitted requests are taken from the head of the FIFO queue into one
   persistent batched launch until the batch's estimated GPU time (algorithmic AES lookups at
   the lookup rate of the kernels) reaches `batch_cap_ms`, so early arrivals are not held back
-  behind everything queued after them; a new batch goes out on a free stream slot while at
-  most `max_inflight - 1` earlier batches are still queued or running, so the device never
-  idles between batches and a request waits behind a bounded amount of work. A request's
+  behind everything queued after them; a new batch is queued (on the stream slots in turn; one
+  slot by default, as every batch spans all SMs) while at most `max_inflight - 1` earlier
+  batches are still queued or running, so the device never idles between batches and a
+  request waits behind a bounded amount of work. Within a batch, requests that fill every SM
+  on their own (DCF requests of >= 148 x 512 elements, spline requests of >= 148 x 16) go out
+  as their own per-call launches in queue order, and only the runs of smaller requests share a
+  persistent batched launch (that is where one launch gains: small requests cannot fill the
+  GPU, while a large one is served best by its dedicated kernel). A request's
   masked input is copied in from pinned host memory and its shares copied back on the same
   stream;
 * records per-request latency (completion - arrival, wall clock; completion is observed by
@@ -195,17 +200,18 @@ def request_lookups(r: Request) -> int:
 
 
 class Server:
-    def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=4, tuning: batch.Tuning | None = None,
+    def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=1, tuning: batch.Tuning | None = None,
                  max_inflight: int = 2, batch_cap_ms: float = 4.0, lookups_per_s: float = 8.0e12):
         self.P = pools
         self.dev = pools.dev
         self.store = KeyStore(capacity_bytes)
         self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
         self.tuning = tuning or batch.Tuning(512, 1 << 26, 0, 0)
-        self.max_inflight = max(1, min(max_inflight, slots))
+        self.max_inflight = max(1, max_inflight)
         self.batch_cap = batch_cap_ms * 1e-3 * lookups_per_s
         self.launches = 0
         self.batch_log: list | None = None  # set to [] to record per-batch host time and kernel events
+        self.sm_threads = torch.cuda.get_device_properties(self.dev).multi_processor_count * 512
 
     def warmup(self) -> None:
         """One request of every size class through both paths, synchronously: loads the kernels
@@ -284,11 +290,49 @@ class Server:
             if was:
                 gc.enable()
 
+    def _fills_gpu(self, r: Request) -> bool:
+        """True if r's own launch already puts a full CTA on every SM (a DCF element is one
+        thread, a spline element one warp)."""
+        return r.size * (1 if r.kind == "dcf" else 32) >= self.sm_threads
+
+    def _launch_plain(self, r: Request, s, t0: float):
+        with torch.cuda.stream(s):
+            keep = self._plain_call(r, s)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self.launches += 1
+        r.start = time.perf_counter() - t0
+        return ev, None, [r], keep
+
+    def _launch_batch(self, rs: list[Request], si: int, t0: float):
+        s = self.slots[si]
+        h0 = time.perf_counter()
+        with torch.cuda.stream(s):
+            reqs = [self._build(r) for r in rs]
+            b = batch.Batch(reqs, self.dev).prepare(self.tuning)
+            if self.batch_log is not None:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+            b.launch()
+            if self.batch_log is not None:
+                e1 = torch.cuda.Event(enable_timing=True)
+                e1.record(s)
+                self.batch_log.append({"requests": len(rs), "lookups": sum(request_lookups(r) for r in rs),
+                                       "host_ms": (time.perf_counter() - h0) * 1e3, "events": (e0, e1)})
+            for r, q in zip(rs, reqs):
+                r.out_host.copy_(q.tensors[0].view(-1), non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self.launches += 1
+        tstart = time.perf_counter() - t0
+        for r in rs:
+            r.start = tstart
+        return ev, si, rs, (b, reqs)
+
     def _run(self, requests: list[Request], mode: str, poll_s: float) -> float:
         pending: deque[Request] = deque()
         arrivals = deque(sorted(requests, key=lambda r: r.arrival))
         inflight = []  # (event, slot index or None, [requests], keep-alive)
-        free = list(range(len(self.slots)))
         done, total = 0, len(requests)
         t0 = time.perf_counter()
         while done < total:
@@ -303,55 +347,35 @@ class Server:
                         r.done = tdone
                         self.store.release(r.key_bytes)
                     done += len(rs)
-                    if si is not None:
-                        free.append(si)
                 else:
                     still.append((ev, si, rs, keep))
             inflight = still
             if mode == "batched":
-                if pending and free and len(inflight) < self.max_inflight:
+                if pending and len(inflight) < self.max_inflight:
                     admitted, cost = [], 0
                     while pending and (not admitted or cost + request_lookups(pending[0]) <= self.batch_cap) \
                             and self.store.try_admit(pending[0].key_bytes):
                         cost += request_lookups(pending[0])
                         admitted.append(pending.popleft())
                     if admitted:
-                        si = free.pop()
-                        s = self.slots[si]
-                        h0 = time.perf_counter()
-                        with torch.cuda.stream(s):
-                            reqs = [self._build(r) for r in admitted]
-                            b = batch.Batch(reqs, self.dev).prepare(self.tuning)
-                            if self.batch_log is not None:
-                                e0 = torch.cuda.Event(enable_timing=True)
-                                e0.record(s)
-                            b.launch()
-                            if self.batch_log is not None:
-                                e1 = torch.cuda.Event(enable_timing=True)
-                                e1.record(s)
-                                self.batch_log.append({"requests": len(admitted), "lookups": cost,
-                                                       "host_ms": (time.perf_counter() - h0) * 1e3,
-                                                       "events": (e0, e1)})
-                            for r, q in zip(admitted, reqs):
-                                r.out_host.copy_(q.tensors[0].view(-1), non_blocking=True)
-                            ev = torch.cuda.Event()
-                            ev.record(s)
-                        self.launches += 1
-                        tstart = time.perf_counter() - t0
-                        for r in admitted:
-                            r.start = tstart
-                        inflight.append((ev, si, admitted, (b, reqs)))
+                        # FIFO order on one stream: runs of requests too small to fill the GPU
+                        # share a persistent launch; a request that fills it alone takes its
+                        # per-call kernel (the batched launch would add nothing but a slower
+                        # generic kernel for it).
+                        si = self.launches % len(self.slots)
+                        run: list[Request] = []
+                        for r in admitted + [None]:
+                            if r is not None and not self._fills_gpu(r):
+                                run.append(r)
+                                continue
+                            if run:
+                                inflight.append(self._launch_batch(run, si, t0))
+                                run = []
+                            if r is not None:
+                                inflight.append(self._launch_plain(r, self.slots[si], t0))
             else:
-                s = self.slots[0]
                 while pending and self.store.try_admit(pending[0].key_bytes):
-                    r = pending.popleft()
-                    with torch.cuda.stream(s):
-                        keep = self._plain_call(r, s)
-                        ev = torch.cuda.Event()
-                        ev.record(s)
-                    self.launches += 1
-                    r.start = time.perf_counter() - t0
-                    inflight.append((ev, None, [r], keep))
+                    inflight.append(self._launch_plain(pending.popleft(), self.slots[0], t0))
             if not (arrivals and arrivals[0].arrival <= time.perf_counter() - t0):
                 time.sleep(poll_s)
         return time.perf_counter() - t0
