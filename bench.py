@@ -534,9 +534,11 @@ def grotto_section(dev, args, peak_glookups) -> dict:
     ok = bool((E.abs() == 1).all() and torch.equal(E * (t[0] + t[2]).view(-1), lut[seg]))
     del rows, rows1, key
     torch.cuda.empty_cache()
+    # every internal node of the depth-(n-6) tree expanded once: key schedule + both children
+    # (40 + 320) less the 14 first-round lookups they share; the parents of leaves skip the 4
+    # last-round lookups of word 1 in each child (no leaf reads it)
     D = n - 6
-    nodes = (1 << D) - 1
-    lookups_per_key = nodes * (40 + 320)
+    lookups_per_key = ((1 << (D - 1)) - 1) * 346 + (1 << (D - 1)) * 338
     ach = lookups_per_key * N / (le_ms / 1e3) / 1e9
     total = le_ms + lut_rows_ms
     return {"workload": ("Grotto full domain over Z_2: 2^16 keys, n=16 (2^16 leaf bits per key, bit-packed), then "

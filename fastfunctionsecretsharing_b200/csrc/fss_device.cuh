@@ -242,6 +242,48 @@ __device__ __forceinline__ void aes_prg_pair(const AesLanes& A, const uint32_t k
     }
 }
 
+// Both children of the GGM node keyed by `key` (blocks 0 and 1: LE64(0) || LE64(1) and
+// LE64(2) || LE64(3)), sharing the 14 first-round lookups their plaintexts have in common. The
+// last round computes only the columns set in MASK (bit c: word c); the others are left 0.
+template <int MASK>
+__device__ __forceinline__ void aes_prg_children(const AesLanes& A, const uint32_t key[4], uint32_t L[4], uint32_t R[4])
+{
+    uint32_t       w[4] = {key[0], key[1], key[2], key[3]};
+    const uint32_t a0 = w[0], b0 = w[0] ^ (2u << 24);
+    const uint32_t a2 = w[2] ^ (1u << 24), b2 = w[2] ^ (3u << 24);
+    const uint32_t s1 = w[1], s3 = w[3];
+    key_step(A, w, 0x01u);
+    const uint32_t x0 = te<1, 2>(A, s1) ^ te<2, 1>(A, a2) ^ te<3, 0>(A, s3) ^ w[0];
+    const uint32_t t1 = te<0, 3>(A, s1) ^ te<1, 2>(A, a2) ^ te<2, 1>(A, s3) ^ te<3, 0>(A, a0) ^ w[1];
+    const uint32_t x2 = te<1, 2>(A, s3) ^ te<2, 1>(A, a0) ^ te<3, 0>(A, s1) ^ w[2];
+    const uint32_t t3 = te<0, 3>(A, s3) ^ te<1, 2>(A, a0) ^ te<2, 1>(A, s1) ^ te<3, 0>(A, a2) ^ w[3];
+    uint32_t       sa[4] = {te<0, 3>(A, a0) ^ x0, t1, te<0, 3>(A, a2) ^ x2, t3};
+    uint32_t       sb[4] = {te<0, 3>(A, b0) ^ x0, t1, te<0, 3>(A, b2) ^ x2, t3};
+    constexpr uint32_t RCON[10] = {0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80, 0x1b, 0x36};
+#pragma unroll
+    for (int r = 1; r < 9; r++)
+    {
+        key_step(A, w, RCON[r]);
+        enc_round(A, sa, w);
+        enc_round(A, sb, w);
+    }
+    key_step(A, w, RCON[9]);
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+    {
+        if (MASK & (1 << c))
+        {
+            L[c] = sub_col(A, sa[c], sa[(c + 1) & 3], sa[(c + 2) & 3], sa[(c + 3) & 3]) ^ w[c];
+            R[c] = sub_col(A, sb[c], sb[(c + 1) & 3], sb[(c + 2) & 3], sb[(c + 3) & 3]) ^ w[c];
+        }
+        else
+        {
+            L[c] = 0;
+            R[c] = 0;
+        }
+    }
+}
+
 // NK independent keys, NB blocks under each. The round loop is not unrolled (small code for
 // the kernels that instantiate several of these); inside an iteration the block rounds under
 // round key r and the schedule step to round key r + 1 are independent, so they overlap.

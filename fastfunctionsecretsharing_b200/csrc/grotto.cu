@@ -202,11 +202,12 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
 // ---------------------------------------------------------------------------------------
 // Full domain. One thread expands a subtree of depth d (2^d leaves) below a node reached by
 // walking the top D - d levels, expanding both children of every internal node once
-// (key schedule + 2 blocks) and keeping right siblings on a small stack. Each leaf j yields
-// the 64-bit word u_j (equality shares of x = 64 j .. 64 j + 63) and the right-turn parity
+// (key schedule + 2 blocks sharing 14 first-round lookups; for the parents of leaves the last
+// round skips word 1, which no leaf reads) and keeping right siblings on a small stack. Each
+// leaf j yields the 64-bit word u_j (equality shares of x = 64 j .. 64 j + 63) and the right-turn parity
 // P_j; the comparison row is excl_prefix_xor(u_j) ^ (P_j ^ party ? ~0 : 0).
 // ---------------------------------------------------------------------------------------
-constexpr int kAllMaxSub = 5;
+constexpr int kAllMaxSub = 7; // 128 leaves per thread (measured best of 5..8 at n = 16)
 
 __device__ __forceinline__ uint64_t excl_prefix_xor(uint64_t u)
 {
@@ -261,10 +262,12 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
                 const uint32_t lv = top + depth;
                 uint32_t       cw[4];
                 load_block_be(K.sCW + 16 * lv, cw);
+                // leaf parents: a leaf reads words 2, 3 (its 64 bits) and word 0 (its control bit)
                 uint32_t st[2][4];
-                prg_block(st[0], 0);
-                prg_block(st[1], 1);
-                aes_encrypt<2>(A, s, st);
+                if (depth + 1 == d)
+                    aes_prg_children<0xD>(A, s, st[0], st[1]);
+                else
+                    aes_prg_children<0xF>(A, s, st[0], st[1]);
                 const uint32_t m  = 0u - t;
                 uint32_t       tL = (st[0][0] >> 24) & 1u, tR = (st[1][0] >> 24) & 1u;
                 st[0][0] &= ~kSeedTBit;

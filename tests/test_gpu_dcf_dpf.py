@@ -184,3 +184,26 @@ def test_staged_eval_partial_tiles(F, oracle, kind, es, n):
     cnt = ctypes.c_uint(7)
     assert _lib.fn("FastFss_b200_stageTimeouts")(ctypes.byref(cnt)) == 0
     assert cnt.value == 0
+
+
+def test_config1_keygen_eval_full_size(F, oracle):
+    """The plain DCF keyGen + eval workload the reference's CPU path is timed on: 2^16 elements,
+    n = 16, output Z_2^16 stored as uint16, seeded alpha, beta, mask m and 128-bit seeds,
+    maskedX = (m + alpha) mod 2^16. GPU keys and both parties' shares equal the oracle's byte
+    for byte, and the shares reconstruct beta * [maskedX < alpha] (the reference's test
+    identity, tests/dcf/dcf_eval_test_case.h)."""
+    rng = np.random.default_rng(20160)
+    N, n, es = 1 << 16, 16, 2
+    a, b, m = rnd(rng, N, es, n), rnd(rng, N, es, n), rnd(rng, N, es, n)
+    s0, s1 = seeds(rng, N), seeds(rng, N)
+    x = ((m.astype(np.uint32) + a.astype(np.uint32)) & 0xFFFF).astype(np.uint16)
+    kref = oracle.dcf_keygen(a, b, s0, s1, n, n, 1)
+    key = _dcf(F, "dcf", a, b, s0, s1, n, n, 1)
+    assert np.array_equal(host(key), kref)
+    y = []
+    for p, s in ((0, s0), (1, s1)):
+        got = _eval(F, "dcf", key, x, s, p, n, n, 1)
+        assert np.array_equal(got, oracle.dcf_eval(x, kref, s, p, n, n, 1))
+        y.append(got.astype(np.uint32))
+    want = np.where(x.astype(np.uint32) < a.astype(np.uint32), b.astype(np.uint32), 0)
+    assert np.array_equal((y[0] + y[1]) & 0xFFFF, want)
