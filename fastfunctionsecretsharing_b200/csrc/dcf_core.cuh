@@ -37,9 +37,13 @@ __device__ __forceinline__ uint32_t dcf_step(const AesLanes &A, uint32_t s[4], u
     uint32_t cw[4];
     load_block_be(cwp, cw);
     uint32_t st[2][4];
-    prg_block(st[0], 2 * dir);
-    prg_block(st[1], 2 * dir + 1);
-    aes_encrypt<2>(A, s, st);
+    {
+        const uint32_t sk[1][4] = {{s[0], s[1], s[2], s[3]}}, d1[1] = {dir};
+        uint32_t       sn[1][4], vv[1][4];
+        aes_prg_pair<1, 4>(A, sk, d1, sn, vv);
+#pragma unroll
+        for (int c = 0; c < 4; c++) st[0][c] = sn[0][c], st[1][c] = vv[0][c];
+    }
     uint32_t       tn = (st[0][0] >> 24) & 1u;
     const uint32_t m  = 0u - t;
     st[0][0] &= ~kSeedTBit;
@@ -237,10 +241,23 @@ __device__ __forceinline__ void dcf_keygen_element(const AesLanes &A, uint8_t *k
     for (uint32_t lv = 0; lv < n; lv++)
     {
         uint32_t G0[4][4], G1[4][4];
-#pragma unroll
-        for (int b = 0; b < 4; b++) prg_block(G0[b], b), prg_block(G1[b], b);
-        aes_encrypt<4>(A, s0, G0);
-        aes_encrypt<4>(A, s1, G1);
+        // groupSize 1 with values of <= 4 (<= 8) bytes reads 1 (2) words of the value blocks
+        const int vw = (g != 1) ? 4 : ((bo + 7) / 8 <= 4 ? 1 : 2);
+        if (vw == 1)
+        {
+            aes_prg_quad<1>(A, s0, G0);
+            aes_prg_quad<1>(A, s1, G1);
+        }
+        else if (vw == 2)
+        {
+            aes_prg_quad<2>(A, s0, G0);
+            aes_prg_quad<2>(A, s1, G1);
+        }
+        else
+        {
+            aes_prg_quad<4>(A, s0, G0);
+            aes_prg_quad<4>(A, s1, G1);
+        }
         const uint32_t tL0 = (G0[0][0] >> 24) & 1u, tR0 = (G0[2][0] >> 24) & 1u;
         const uint32_t tL1 = (G1[0][0] >> 24) & 1u, tR1 = (G1[2][0] >> 24) & 1u;
         G0[0][0] &= ~kSeedTBit, G0[2][0] &= ~kSeedTBit, G1[0][0] &= ~kSeedTBit, G1[2][0] &= ~kSeedTBit;
@@ -264,24 +281,43 @@ __device__ __forceinline__ void dcf_keygen_element(const AesLanes &A, uint8_t *k
 #pragma unroll
         for (int c = 0; c < 4; c++) sCW[c] = sLose0[c] ^ sLose1[c];
 
-        ConvertStream cL1, cL0, cK1, cK0;
-        cL1.init(vLose1, g, bo);
-        cL0.init(vLose0, g, bo);
-        cK1.init(vKeep1, g, bo);
-        cK0.init(vKeep0, g, bo);
-        for (uint32_t j = 0; j < g; j++)
+        if (g == 1)
         {
-            uint64_t va = (uint64_t)last[j];
-            uint64_t v  = cL1.value(A, j) - cL0.value(A, j) - va;
+            // groupSize 1: the convert is the first ceil(bo/8) bytes of the value block
+            const int      ges = (int)((bo + 7) / 8);
+            uint64_t       va  = (uint64_t)last[0];
+            uint64_t       v   = block_le_prefix(vLose1, ges) - block_le_prefix(vLose0, ges) - va;
             if (t1) v = 0 - v;
             if (keep)
             {
-                const uint64_t b = beta ? (uint64_t)beta[j] : (uint64_t)(j == 0);
+                const uint64_t b = beta ? (uint64_t)beta[0] : 1u;
                 v += t1 ? (0 - b) : b;
             }
-            vCW[(size_t)lv * g + j] = (GE)v;
-            va                      = va - cK1.value(A, j) + cK0.value(A, j) + (t1 ? (0 - v) : v);
-            last[j]                 = (GE)va;
+            vCW[lv] = (GE)v;
+            va      = va - block_le_prefix(vKeep1, ges) + block_le_prefix(vKeep0, ges) + (t1 ? (0 - v) : v);
+            last[0] = (GE)va;
+        }
+        else
+        {
+            ConvertStream cL1, cL0, cK1, cK0;
+            cL1.init(vLose1, g, bo);
+            cL0.init(vLose0, g, bo);
+            cK1.init(vKeep1, g, bo);
+            cK0.init(vKeep0, g, bo);
+            for (uint32_t j = 0; j < g; j++)
+            {
+                uint64_t va = (uint64_t)last[j];
+                uint64_t v  = cL1.value(A, j) - cL0.value(A, j) - va;
+                if (t1) v = 0 - v;
+                if (keep)
+                {
+                    const uint64_t b = beta ? (uint64_t)beta[j] : (uint64_t)(j == 0);
+                    v += t1 ? (0 - b) : b;
+                }
+                vCW[(size_t)lv * g + j] = (GE)v;
+                va                      = va - cK1.value(A, j) + cK0.value(A, j) + (t1 ? (0 - v) : v);
+                last[j]                 = (GE)va;
+            }
         }
 
         store_block_be(sCWp + 16 * lv, sCW);
@@ -302,6 +338,14 @@ __device__ __forceinline__ void dcf_keygen_element(const AesLanes &A, uint8_t *k
     }
     tLp[0] = (GE)tl;
     tLp[1] = (GE)tr;
+    if (g == 1)
+    {
+        const int ges = (int)((bo + 7) / 8);
+        uint64_t  v   = block_le_prefix(s1, ges) - block_le_prefix(s0, ges) - (uint64_t)last[0];
+        if (t1) v = 0 - v;
+        last[0] = (GE)v;
+        return;
+    }
     ConvertStream c1, c0;
     c1.init(s1, g, bo);
     c0.init(s0, g, bo);

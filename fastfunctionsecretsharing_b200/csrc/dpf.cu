@@ -47,9 +47,8 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
         for (uint32_t lv = 0; lv < n; lv++)
         {
             uint32_t G0[2][4], G1[2][4];
-            prg_block(G0[0], 0), prg_block(G0[1], 1), prg_block(G1[0], 0), prg_block(G1[1], 1);
-            aes_encrypt<2>(A, s0, G0);
-            aes_encrypt<2>(A, s1, G1);
+            aes_prg_children<0xF>(A, s0, G0[0], G0[1]);
+            aes_prg_children<0xF>(A, s1, G1[0], G1[1]);
             const uint32_t tL0 = (G0[0][0] >> 24) & 1u, tR0 = (G0[1][0] >> 24) & 1u;
             const uint32_t tL1 = (G1[0][0] >> 24) & 1u, tR1 = (G1[1][0] >> 24) & 1u;
             G0[0][0] &= ~kSeedTBit, G0[1][0] &= ~kSeedTBit, G1[0][0] &= ~kSeedTBit, G1[1][0] &= ~kSeedTBit;
