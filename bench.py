@@ -298,14 +298,15 @@ def main():
     value = N * world * args.steps / (total_ms / 1e3) / 1e9
 
     # ---- end to end through the public API, host buffers, H2D + D2H per step ----
-    # Every step copies its maskedX in from pinned host memory and its shares back out; two
-    # device buffers let step i's copies overlap step i-1's evaluation (copy stream + compute
-    # stream, ordered by events).
+    # Every step copies its maskedX in from pinned host memory and its shares back out. Two
+    # device buffers and separate H2D and D2H copy streams (ordered by events) let step i + 1's
+    # input copy and step i - 1's output copy run while step i is evaluated.
     host_x = masked.cpu().pin_memory()
     host_out = [torch.empty(N, dtype=torch.int32).pin_memory() for _ in range(2)]
     dev_x = [torch.empty_like(masked) for _ in range(2)]
     dev_out = [torch.empty(0, dtype=torch.int32, device=dev) for _ in range(2)]
-    copy_stream = torch.cuda.Stream(dev)
+    h2d_stream = torch.cuda.Stream(dev)
+    copy_stream = torch.cuda.Stream(dev)  # device -> host
     h2d_done = [torch.cuda.Event() for _ in range(2)]
     comp_done = [torch.cuda.Event() for _ in range(2)]
     d2h_done = [torch.cuda.Event() for _ in range(2)]
@@ -313,12 +314,14 @@ def main():
     def e2e_steps(k):
         for i in range(k):
             b = i % 2
-            with torch.cuda.stream(copy_stream):
+            with torch.cuda.stream(h2d_stream):
                 if i >= 2:
-                    copy_stream.wait_event(d2h_done[b])
+                    h2d_stream.wait_event(comp_done[b])  # dev_x[b] was read by step i - 2
                 dev_x[b].copy_(host_x, non_blocking=True)
-                h2d_done[b].record(copy_stream)
+                h2d_done[b].record(h2d_stream)
             stream.wait_event(h2d_done[b])
+            if i >= 2:
+                stream.wait_event(d2h_done[b])  # dev_out[b] was copied out by step i - 2
             F.dcf_eval(dev_out[b], dev_x[b], key, seed0, 0, N_BITS, N_BITS, 1)
             comp_done[b].record(stream)
             with torch.cuda.stream(copy_stream):
@@ -332,10 +335,12 @@ def main():
     torch.cuda.synchronize(dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(copy_stream)
+    e0.record(h2d_stream)
     stream.wait_event(e0)
+    copy_stream.wait_event(e0)
     e2e_steps(args.steps)
     copy_stream.wait_stream(stream)
+    copy_stream.wait_stream(h2d_stream)
     e1.record(copy_stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -409,8 +414,9 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N * ES, "d2h_bytes_per_step": N * ES,
                 "shares_match_device_run": e2e_ok,
                 "note": ("public API (fastfunctionsecretsharing_b200.dcf_eval -> FastFss_cuda_dcfEval); each step copies "
-                         "maskedX in from pinned host memory and the shares out; copies of one step overlap the "
-                         "evaluation of the previous one (two buffers); keys/seeds stay device-resident")},
+                         "maskedX in from pinned host memory and the shares out; a step's input and output copies "
+                         "overlap the neighbouring steps' evaluations (two buffers, separate H2D and D2H streams); "
+                         "keys/seeds stay device-resident")},
         "gpu_launches": args.steps,
         "gpu_launches_e2e": args.steps,
         "clocks": ck,
