@@ -382,6 +382,91 @@ __device__ __forceinline__ void aes_encrypt_keys(const AesLanes& A, const uint32
     }
 }
 
+// Two independent groups in the same rounds: N1 keys with B1 blocks each and N2 keys with B2
+// blocks each (e.g. the next tree level of a walk together with the value convert of the level
+// before it, which do not depend on each other). Rolled rounds, as aes_encrypt_keys.
+template <int N1, int B1, int N2, int B2>
+__device__ __forceinline__ void aes_encrypt_groups(const AesLanes& A, const uint32_t k1[N1][4], uint32_t st1[N1][B1][4],
+                                                   const uint32_t k2[N2][4], uint32_t st2[N2][B2][4])
+{
+    uint32_t w1[N1][4], w2[N2][4];
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) w1[k][c] = k1[k][c];
+#pragma unroll
+        for (int b = 0; b < B1; b++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) st1[k][b][c] ^= w1[k][c];
+        }
+        key_step(A, w1[k], 0x01u);
+    }
+#pragma unroll
+    for (int k = 0; k < N2; k++)
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) w2[k][c] = k2[k][c];
+#pragma unroll
+        for (int b = 0; b < B2; b++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) st2[k][b][c] ^= w2[k][c];
+        }
+        key_step(A, w2[k], 0x01u);
+    }
+    uint32_t rcon = 0x01u;
+#pragma unroll 1
+    for (int r = 1; r < 10; r++)
+    {
+        rcon = gf_xtime(rcon);
+        uint32_t n1[N1][4], n2[N2][4];
+#pragma unroll
+        for (int k = 0; k < N1; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) n1[k][c] = w1[k][c];
+            key_step(A, n1[k], rcon);
+#pragma unroll
+            for (int b = 0; b < B1; b++) enc_round(A, st1[k][b], w1[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) n2[k][c] = w2[k][c];
+            key_step(A, n2[k], rcon);
+#pragma unroll
+            for (int b = 0; b < B2; b++) enc_round(A, st2[k][b], w2[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < N1; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) w1[k][c] = n1[k][c];
+        }
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) w2[k][c] = n2[k][c];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+    {
+#pragma unroll
+        for (int b = 0; b < B1; b++) enc_last(A, st1[k][b], w1[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < N2; k++)
+    {
+#pragma unroll
+        for (int b = 0; b < B2; b++) enc_last(A, st2[k][b], w2[k]);
+    }
+}
+
 // PRG block j of the GGM expansion: plaintext = LE64(2j) || LE64(2j+1) as BE words.
 __device__ __forceinline__ void prg_block(uint32_t st[4], uint32_t j)
 {

@@ -3,11 +3,12 @@
 // persistent kernel. Algorithm: src/impl/spline.h:186-253 of the reference.
 //
 // Lane lg of element i takes intervals q = lg, lg + G, ... . For interval q it walks the two
-// DCF paths x - 1 - L_q and x - 1 - (R_q + 1) side by side (one AES call carries both paths'
-// blocks, so a level issues twice the independent lookups), and reads only slot q's values
-// out of each level's convert stream: the value bytes j0 ges .. (j0 + cnt) ges - 1 lie in at
-// most three consecutive 16-byte blocks of the AES-CTR stream, which are encrypted under one
-// key schedule and read with register masks (no dynamically indexed arrays).
+// DCF paths x - 1 - L_q and x - 1 - (R_q + 1) side by side, and reads only slot q's values out
+// of each level's convert stream: the value bytes j0 ges .. (j0 + cnt) ges - 1 lie in at most
+// three consecutive 16-byte blocks of the AES-CTR stream, which are encrypted under one key
+// schedule and read with register masks (no dynamically indexed arrays). Each AES call carries
+// the next level of both walks and the previous level's converts (independent work, so the
+// rounds have 4 + 2 NB blocks in flight).
 #pragma once
 
 #include "dcf_core.cuh"
@@ -56,40 +57,32 @@ __device__ __forceinline__ uint32_t spline_window_blocks(uint32_t m, uint32_t cn
     return nb;
 }
 
-// Adds the shares of values j0 .. j0 + cnt - 1 of the two convert streams keyed by key[0] and
-// key[1] (with the correction corr[j0 + c] where tc[k] is set) into acc[k][c].
-template <typename GE, int NB, bool AES>
-__device__ __forceinline__ void spline_slot_add(const AesLanes &A, const uint32_t key[2][4], const uint32_t tc[2],
-                                                const GE *corr, uint32_t party, uint32_t ges, uint32_t off,
-                                                const uint32_t ctr[NB], uint32_t j0, uint32_t cnt,
-                                                uint64_t acc[2][kSplineMaxC])
+// Counter blocks of the convert stream for the slot window (blocks ctr[0 .. NB)).
+template <int NB>
+__device__ __forceinline__ void slot_counters(uint32_t W[2][NB][4], const uint32_t ctr[NB])
 {
-    uint32_t W[2][NB][4];
-    if (AES)
+#pragma unroll
+    for (int k = 0; k < 2; k++)
     {
 #pragma unroll
-        for (int k = 0; k < 2; k++)
+        for (int b = 0; b < NB; b++)
         {
-#pragma unroll
-            for (int b = 0; b < NB; b++)
-            {
-                W[k][b][0] = 0;
-                W[k][b][1] = 0;
-                W[k][b][2] = bswap32(ctr[b]);
-                W[k][b][3] = 0;
-            }
-        }
-        aes_encrypt_keys<2, NB>(A, key, W);
-    }
-    else
-    {
-#pragma unroll
-        for (int k = 0; k < 2; k++)
-        {
-#pragma unroll
-            for (int c = 0; c < 4; c++) W[k][0][c] = key[k][c];
+            W[k][b][0] = 0;
+            W[k][b][1] = 0;
+            W[k][b][2] = bswap32(ctr[b]);
+            W[k][b][3] = 0;
         }
     }
+}
+
+// Adds the shares of values j0 .. j0 + cnt - 1 read out of the windows W[k] (the encrypted
+// slot blocks of convert stream k, or for a stream that needs no AES its key block itself in
+// W[k][0]) into acc[k][c], with the correction corr[j0 + c] where tc[k] is set.
+template <typename GE, int NB>
+__device__ __forceinline__ void slot_accumulate(const uint32_t W[2][NB][4], const uint32_t tc[2], const GE *corr,
+                                                uint32_t party, uint32_t ges, uint32_t off, uint32_t j0,
+                                                uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+{
     uint64_t cv[kSplineMaxC];
 #pragma unroll
     for (int c = 0; c < kSplineMaxC; c++) cv[c] = ((uint32_t)c < cnt) ? (uint64_t)__ldg(corr + j0 + c) : 0;
@@ -110,7 +103,33 @@ __device__ __forceinline__ void spline_slot_add(const AesLanes &A, const uint32_
     }
 }
 
-// Both DCF walks of one interval (points xa, xb), slot values j0 .. j0 + cnt - 1.
+// Seeds and control bits of both walks after the node expansion st (children of s[k] along
+// dir[k]); the value children go to v.
+__device__ __forceinline__ void walk_advance(uint32_t s[2][4], uint32_t t[2], uint32_t v[2][4],
+                                             uint32_t st[2][2][4], const uint32_t dir[2], const uint32_t cw[4],
+                                             uint64_t tl, uint64_t tr, uint32_t lv)
+{
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+    {
+        uint32_t       tn = (st[k][0][0] >> 24) & 1u;
+        const uint32_t mk = 0u - t[k];
+        st[k][0][0] &= ~kSeedTBit;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+        {
+            s[k][c] = st[k][0][c] ^ (cw[c] & mk);
+            v[k][c] = st[k][1][c];
+        }
+        tn ^= (uint32_t)(((dir[k] ? tr : tl) >> lv) & 1u) & t[k];
+        t[k] = tn;
+    }
+}
+
+// Both DCF walks of one interval (points xa, xb), slot values j0 .. j0 + cnt - 1. The walk is
+// software pipelined: one AES call expands level lv + 1 of both walks (2 keys x 2 blocks) and
+// encrypts the slot blocks of level lv's value convert (2 keys x NB blocks), which do not
+// depend on each other, so every round carries 2 (2 + NB) independent block rounds.
 template <typename GE, int NB, bool AES>
 __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
                                                  uint32_t party, uint32_t n, uint32_t g, uint32_t ges, uint64_t xa,
@@ -128,12 +147,13 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
 #pragma unroll
     for (int c = 0; c < 4; c++) s[1][c] = s[0][c];
     uint32_t t[2] = {party, party};
-#pragma unroll 1
-    for (uint32_t lv = 0; lv < n; lv++)
+
+    // level 0 alone
+    uint32_t v[2][4], tp[2] = {party, party};
     {
         uint32_t cw[4];
-        load_block_be(K.sCW + 16 * lv, cw);
-        const uint32_t dir[2] = {(uint32_t)((xa >> (n - 1 - lv)) & 1u), (uint32_t)((xb >> (n - 1 - lv)) & 1u)};
+        load_block_be(K.sCW, cw);
+        const uint32_t dir[2] = {(uint32_t)((xa >> (n - 1)) & 1u), (uint32_t)((xb >> (n - 1)) & 1u)};
         uint32_t       st[2][2][4];
 #pragma unroll
         for (int k = 0; k < 2; k++)
@@ -141,29 +161,62 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
             prg_block(st[k][0], 2 * dir[k]);
             prg_block(st[k][1], 2 * dir[k] + 1);
         }
-        // rolled rounds (aes_encrypt_keys): the unrolled shared-first-round form (aes_prg_pair)
-        // measured 5 % slower here (code size), despite 14 fewer lookups per walk and level
         aes_encrypt_keys<2, 2>(A, s, st);
-        uint32_t v[2][4], tp[2];
+        walk_advance(s, t, v, st, dir, cw, K.tl, K.tr, 0);
+    }
+#pragma unroll 1
+    for (uint32_t lv = 0; lv + 1 < n; lv++)
+    {
+        // holds: v, tp = value child and parent control bit of level lv; s, t at level lv + 1
+        const uint32_t l1 = lv + 1;
+        uint32_t       cw[4];
+        load_block_be(K.sCW + 16 * l1, cw);
+        const uint32_t dir[2] = {(uint32_t)((xa >> (n - 1 - l1)) & 1u), (uint32_t)((xb >> (n - 1 - l1)) & 1u)};
+        uint32_t       st[2][2][4], W[2][NB][4];
 #pragma unroll
         for (int k = 0; k < 2; k++)
         {
-            tp[k]            = t[k];
-            uint32_t       tn = (st[k][0][0] >> 24) & 1u;
-            const uint32_t mk = 0u - t[k];
-            st[k][0][0] &= ~kSeedTBit;
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-            {
-                s[k][c] = st[k][0][c] ^ (cw[c] & mk);
-                v[k][c] = st[k][1][c];
-            }
-            tn ^= (uint32_t)(((dir[k] ? K.tr : K.tl) >> lv) & 1u) & t[k];
-            t[k] = tn;
+            prg_block(st[k][0], 2 * dir[k]);
+            prg_block(st[k][1], 2 * dir[k] + 1);
         }
-        spline_slot_add<GE, NB, AES>(A, v, tp, K.vCW + (size_t)lv * g, party, ges, off, ctr, j0, cnt, acc);
+        if (AES)
+        {
+            slot_counters<NB>(W, ctr);
+            aes_encrypt_groups<2, 2, 2, NB>(A, s, st, v, W);
+        }
+        else
+        {
+            aes_encrypt_keys<2, 2>(A, s, st);
+#pragma unroll
+            for (int k = 0; k < 2; k++)
+            {
+#pragma unroll
+                for (int c = 0; c < 4; c++) W[k][0][c] = v[k][c];
+            }
+        }
+        slot_accumulate<GE, NB>(W, tp, K.vCW + (size_t)lv * g, party, ges, off, j0, cnt, acc);
+        tp[0] = t[0], tp[1] = t[1];
+        walk_advance(s, t, v, st, dir, cw, K.tl, K.tr, l1);
     }
-    spline_slot_add<GE, NB, AES>(A, s, t, K.last, party, ges, off, ctr, j0, cnt, acc);
+    // level n - 1's convert and the leaf convert (keyed by the final seeds) together
+    uint32_t W[2][NB][4], WL[2][NB][4];
+    if (AES)
+    {
+        slot_counters<NB>(W, ctr);
+        slot_counters<NB>(WL, ctr);
+        aes_encrypt_groups<2, NB, 2, NB>(A, v, W, s, WL);
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+#pragma unroll
+            for (int c = 0; c < 4; c++) W[k][0][c] = v[k][c], WL[k][0][c] = s[k][c];
+        }
+    }
+    slot_accumulate<GE, NB>(W, tp, K.vCW + (size_t)(n - 1) * g, party, ges, off, j0, cnt, acc);
+    slot_accumulate<GE, NB>(WL, t, K.last, party, ges, off, j0, cnt, acc);
 }
 
 // The group sums w_c += cx beta_qc - s_qc + s'_qc + e_qc are reduced with shuffles and lane 0
