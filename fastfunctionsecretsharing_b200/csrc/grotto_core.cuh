@@ -98,6 +98,67 @@ __device__ __forceinline__ uint32_t grotto_cmp(const AesLanes &A, const GrottoKe
     return par ^ (uint32_t)(__popcll(u & mask) & 1) ^ party;
 }
 
+// grotto_cmp at two points x[0], x[1] under one key, both walks in the same AES calls (a walk
+// that stops early keeps its state while the other goes on).
+template <typename GE>
+__device__ __forceinline__ void grotto_cmp2(const AesLanes &A, const GrottoKeyView<GE> &K, const uint8_t *seed,
+                                            uint32_t party, uint32_t n, const uint64_t x[2], bool equalBound,
+                                            uint32_t share[2])
+{
+    uint32_t s[2][4];
+    load_block_be(seed, s[0]);
+    s[0][0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++) s[1][c] = s[0][c];
+    uint32_t t[2] = {party, party}, par[2] = {0, 0};
+    bool     early[2] = {false, false};
+#pragma unroll 1
+    for (uint32_t lv = 0; lv + 6 < n; lv++)
+    {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (equalBound && !early[k] && mod_bits<GE>(x[k], n - lv) == 0) early[k] = true;
+        if (early[0] && early[1]) break;
+        uint32_t cw[4];
+        load_block_be(K.sCW + 16 * lv, cw);
+        uint32_t dir[2], st[2][1][4];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            dir[k] = (uint32_t)((x[k] >> (n - 1 - lv)) & 1u);
+            prg_block(st[k][0], dir[k]);
+        }
+        aes_encrypt_keys<2, 1>(A, s, st);
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+        {
+            if (early[k]) continue;
+            uint32_t       tn = (st[k][0][0] >> 24) & 1u;
+            const uint32_t m  = 0u - t[k];
+            st[k][0][0] &= ~kSeedTBit;
+#pragma unroll
+            for (int c = 0; c < 4; c++) s[k][c] = st[k][0][c] ^ (cw[c] & m);
+            tn ^= (uint32_t)(((dir[k] ? K.tr : K.tl) >> lv) & 1u) & t[k];
+            par[k] ^= dir[k] & (t[k] ^ tn);
+            t[k] = tn;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+    {
+        if (early[k])
+        {
+            share[k] = par[k] ^ party;
+            continue;
+        }
+        const uint64_t u0   = hi_u64(s[k]);
+        const uint64_t u    = t[k] ? (u0 ^ K.last) : u0;
+        const uint32_t pre  = (uint32_t)(x[k] & 63u);
+        const uint64_t mask = equalBound ? (pre ? (~0ull >> (64 - pre)) : 0ull) : (~0ull >> (63 - pre));
+        share[k]            = par[k] ^ (uint32_t)(__popcll(u & mask) & 1) ^ party;
+    }
+}
+
 // Interval endpoints shared by MIC and the LUT (src/impl/grotto.h:414-423,499-517):
 // sp = share of [x - (L - 1) <= alpha'], sq = share of [x - R <= alpha'], bit = sp ^ sq ^
 // party [xQ >= xP] (the reference reuses sq of interval i-1 as sp of interval i when the
@@ -109,9 +170,10 @@ __device__ __forceinline__ uint32_t grotto_interval_bit(const AesLanes &A, const
 {
     const uint64_t xP = mod_bits<GE>((uint64_t)(GE)(mx - (uint64_t)(GE)(L - 1)), n);
     const uint64_t xQ = mod_bits<GE>((uint64_t)(GE)(mx - R), n);
-    const uint32_t sp = grotto_cmp<GE>(A, K, seed, party, n, xP, true);
-    const uint32_t sq = grotto_cmp<GE>(A, K, seed, party, n, xQ, true);
-    return (sp ^ sq ^ ((xQ >= xP) ? party : 0u)) & 1u;
+    const uint64_t xs[2] = {xP, xQ};
+    uint32_t       sh[2];
+    grotto_cmp2<GE>(A, K, seed, party, n, xs, true, sh);
+    return (sh[0] ^ sh[1] ^ ((xQ >= xP) ? party : 0u)) & 1u;
 }
 
 } // namespace fss
