@@ -219,6 +219,140 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
     slot_accumulate<GE, NB>(WL, t, K.last, party, ges, off, j0, cnt, acc);
 }
 
+// As slot_accumulate for two windows of ONE convert stream: window w is blocks
+// [w NB, w NB + NB) of W (a stream that needs no AES: its key block W[0] for both), read at byte
+// offset off[w] for values j0[w] .. j0[w] + cnt - 1, into acc[w][c].
+template <typename GE, int NB, bool AES>
+__device__ __forceinline__ void slot_accumulate2(const uint32_t W[][4], uint32_t tc, const GE *corr, uint32_t party,
+                                                 uint32_t ges, const uint32_t off[2], const uint32_t j0[2],
+                                                 uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+{
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+    {
+        uint64_t D[2 * NB];
+        window_words<NB>(W + (AES ? w * NB : 0), D);
+#pragma unroll
+        for (int c = 0; c < kSplineMaxC; c++)
+        {
+            if ((uint32_t)c < cnt)
+            {
+                const uint64_t val = window_value<NB>(D, off[w] + (uint32_t)c * ges, ges) +
+                                     (tc ? (uint64_t)__ldg(corr + j0[w] + c) : 0);
+                acc[w][c] += party ? (0 - val) : val;
+            }
+        }
+    }
+}
+
+// When the intervals tile the ring (R_{q-1} + 1 = L_q for every q, cyclically), the left
+// endpoint point x - 1 - L_q of interval q is also the right endpoint point of interval q - 1,
+// so one DCF walk serves both: it reads slot q (window 0, into acc[0]) and slot q - 1
+// (window 1, into acc[1]) of every level's convert stream, both under the one key schedule of
+// that stream. Software pipelined like spline_walk_pair: each AES call carries the next level
+// (1 key x 2 blocks) and the previous level's convert (1 key x 2 NB blocks).
+template <typename GE, int NB, bool AES>
+__device__ __forceinline__ void spline_walk_shared(const AesLanes &A, const DcfKeyView<GE> &K, const uint8_t *seed,
+                                                   uint32_t party, uint32_t n, uint32_t g, uint32_t ges, uint64_t xp,
+                                                   uint32_t j0a, uint32_t j0b, uint32_t cnt,
+                                                   uint64_t acc[2][kSplineMaxC])
+{
+    const uint32_t j0[2] = {j0a, j0b};
+    uint32_t       off[2], ctr[2][NB];
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+    {
+        const uint32_t start = j0[w] * ges;
+        const uint32_t blo   = AES ? (start >> 4) : 0u;
+        off[w]               = start - 16u * blo;
+#pragma unroll
+        for (int b = 0; b < NB; b++) ctr[w][b] = (16u * (blo + (uint32_t)b)) / ges;
+    }
+    constexpr int WB = AES ? 2 * NB : 1; // blocks per convert
+    uint32_t      s[1][4];
+    load_block_be(seed, s[0]);
+    s[0][0] &= ~kSeedTBit;
+    uint32_t t = party, tp = party, v[1][4];
+    auto advance = [&](uint32_t st[1][2][4], uint32_t dir, const uint32_t cw[4], uint32_t lv) {
+        uint32_t       tn = (st[0][0][0] >> 24) & 1u;
+        const uint32_t mk = 0u - t;
+        st[0][0][0] &= ~kSeedTBit;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+        {
+            s[0][c] = st[0][0][c] ^ (cw[c] & mk);
+            v[0][c] = st[0][1][c];
+        }
+        tn ^= (uint32_t)(((dir ? K.tr : K.tl) >> lv) & 1u) & t;
+        t = tn;
+    };
+    auto counters = [&](uint32_t W[WB][4]) {
+#pragma unroll
+        for (int w = 0; w < 2; w++)
+        {
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+            {
+                W[w * NB + b][0] = 0;
+                W[w * NB + b][1] = 0;
+                W[w * NB + b][2] = bswap32(ctr[w][b]);
+                W[w * NB + b][3] = 0;
+            }
+        }
+    };
+    {
+        uint32_t cw[4];
+        load_block_be(K.sCW, cw);
+        const uint32_t dir = (uint32_t)((xp >> (n - 1)) & 1u);
+        uint32_t       st[1][2][4];
+        prg_block(st[0][0], 2 * dir);
+        prg_block(st[0][1], 2 * dir + 1);
+        aes_encrypt_keys<1, 2>(A, s, st);
+        advance(st, dir, cw, 0);
+    }
+#pragma unroll 1
+    for (uint32_t lv = 0; lv + 1 < n; lv++)
+    {
+        const uint32_t l1 = lv + 1;
+        uint32_t       cw[4];
+        load_block_be(K.sCW + 16 * l1, cw);
+        const uint32_t dir = (uint32_t)((xp >> (n - 1 - l1)) & 1u);
+        uint32_t       st[1][2][4], W[1][WB][4];
+        prg_block(st[0][0], 2 * dir);
+        prg_block(st[0][1], 2 * dir + 1);
+        if (AES)
+        {
+            counters(W[0]);
+            aes_encrypt_groups<1, 2, 1, WB>(A, s, st, v, W);
+        }
+        else
+        {
+            aes_encrypt_keys<1, 2>(A, s, st);
+#pragma unroll
+            for (int c = 0; c < 4; c++) W[0][0][c] = v[0][c];
+        }
+        slot_accumulate2<GE, NB, AES>(W[0], tp, K.vCW + (size_t)lv * g, party, ges, off, j0, cnt, acc);
+        tp = t;
+        advance(st, dir, cw, l1);
+    }
+    // level n - 1's convert and the leaf convert (keyed by the final seed) together
+    uint32_t W[2][WB][4];
+    if (AES)
+    {
+        counters(W[0]);
+        counters(W[1]);
+        const uint32_t keys[2][4] = {{v[0][0], v[0][1], v[0][2], v[0][3]}, {s[0][0], s[0][1], s[0][2], s[0][3]}};
+        aes_encrypt_keys<2, WB>(A, keys, W);
+    }
+    else
+    {
+#pragma unroll
+        for (int c = 0; c < 4; c++) W[0][0][c] = v[0][c], W[1][0][c] = s[0][c];
+    }
+    slot_accumulate2<GE, NB, AES>(W[0], tp, K.vCW + (size_t)(n - 1) * g, party, ges, off, j0, cnt, acc);
+    slot_accumulate2<GE, NB, AES>(W[1], t, K.last, party, ges, off, j0, cnt, acc);
+}
+
 // The group sums w_c += cx beta_qc - s_qc + s'_qc + e_qc are reduced with shuffles and lane 0
 // writes sum_c w_c x^c mod 2^bitWidthOut.
 template <typename GE>
@@ -237,6 +371,15 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
     {
         K.set(key, n, g, i, N);
         x = mod_bits<GE>((uint64_t)__ldg(maskedX + i), n);
+    }
+    // intervals that tile the ring cyclically share endpoint walks (spline_walk_shared);
+    // the same answer for every lane of the group
+    bool contig = true;
+    for (uint32_t q = 0; q < m && contig; q++)
+    {
+        const uint64_t Lq    = mod_bits<GE>((uint64_t)__ldg(left + q), n);
+        const uint64_t Rprev = mod_bits<GE>((uint64_t)__ldg(right + (q == 0 ? m - 1 : q - 1)), n);
+        contig               = mod_bits<GE>((uint64_t)(GE)(Rprev + 1), n) == Lq;
     }
     uint64_t result = 0, xpow = 1;
     for (uint32_t c0 = 0; c0 < cn; c0 += kSplineMaxC)
@@ -260,7 +403,22 @@ __device__ __forceinline__ void spline_eval_group(const AesLanes &A, GE *out, co
 #pragma unroll
                 for (int k = 0; k < kSplineMaxC; k++) w[0][k] = 0, w[1][k] = 0;
                 const uint8_t *sd = seed + 16 * i;
-                if (!aes)
+                if (contig)
+                {
+                    // w[0] = slot q at x - 1 - L_q (this interval's left endpoint); w[1] = slot
+                    // q - 1 at the same point, the right endpoint of interval q - 1. Their sum
+                    // over all q equals the per-interval sum of the pair walks.
+                    const uint32_t jb = (q == 0 ? m - 1 : q - 1) * cn + c0;
+                    if (!aes)
+                        spline_walk_shared<GE, 1, false>(A, K, sd, party, n, g, ges, xa, j0, jb, cnt, w);
+                    else if (nb == 1)
+                        spline_walk_shared<GE, 1, true>(A, K, sd, party, n, g, ges, xa, j0, jb, cnt, w);
+                    else if (nb == 2)
+                        spline_walk_shared<GE, 2, true>(A, K, sd, party, n, g, ges, xa, j0, jb, cnt, w);
+                    else
+                        spline_walk_shared<GE, 3, true>(A, K, sd, party, n, g, ges, xa, j0, jb, cnt, w);
+                }
+                else if (!aes)
                     spline_walk_pair<GE, 1, false>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);
                 else if (nb == 1)
                     spline_walk_pair<GE, 1, true>(A, K, sd, party, n, g, ges, xa, xb, j0, cnt, w);

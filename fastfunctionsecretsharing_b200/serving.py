@@ -192,7 +192,7 @@ def make_requests(P: Pools, rate: float, count: int, seed: int = 1, dcf_log2=(10
 
 # Estimated evaluation cost (AES table lookups) per element, used to cap a batch's GPU time.
 DCF_LOOKUPS = DCF_N * dcf_level_lookups(DCF_N)
-SPLINE_LOOKUPS = algorithmic_lookups("spline", 1, SPLINE_N, SPLINE_N, SPLINE_M, SPLINE_D)
+SPLINE_LOOKUPS = algorithmic_lookups("spline", 1, SPLINE_N, SPLINE_N, SPLINE_M, SPLINE_D, tiling=True)
 
 
 def request_lookups(r: Request) -> int:

@@ -93,25 +93,30 @@ def spline_window_blocks(m: int, cn: int, c0: int, cnt: int, ges: int) -> int:
     return nb
 
 
-def algorithmic_lookups(kind: str, N: int, n: int, bo: int, m: int = 0, d: int = 0) -> int:
+def algorithmic_lookups(kind: str, N: int, n: int, bo: int, m: int = 0, d: int = 0, tiling: bool = False) -> int:
     """AES table lookups one party's evaluation needs.
 
     mic: 2 m groupSize-1 DCF walks of n levels per element.
     spline: per element and interval, two DCF walks of n levels; a level is the node expansion
     (key schedule + seed child + full value child, 346) and the convert of interval q's d + 1
     values out of the value child's AES-CTR stream (key schedule + the blocks holding them);
-    the leaf adds one more convert per walk. Values are read 4 at a time."""
+    the leaf adds one more convert per walk. Values are read 4 at a time. With `tiling`
+    (intervals that tile the ring, R_{q-1} + 1 = L_q) the left endpoint of interval q is the
+    right endpoint of interval q - 1: one walk per interval, whose converts read two slot
+    windows (slots q and q - 1) under one key schedule."""
     if kind == "mic":
         return N * m * 2 * n * dcf_level_lookups(bo)
     if kind == "spline":
         cn, ges = d + 1, (bo + 7) // 8
         g = m * cn
+        windows = 2 if tiling else 1
         conv = 0
         for c0 in range(0, cn, 4):
             cnt = min(4, cn - c0)
-            conv += (40 + 160 * spline_window_blocks(m, cn, c0, cnt, ges)) if ges * g > 16 else 0
+            conv += (40 + 160 * windows * spline_window_blocks(m, cn, c0, cnt, ges)) if ges * g > 16 else 0
         steps = 1 + (cn - 1) // 4  # the walks are repeated per pass of 4 coefficients
-        return N * m * 2 * (steps * n * 346 + (n + 1) * conv)
+        walks = 1 if tiling else 2
+        return N * m * walks * (steps * n * 346 + (n + 1) * conv)
     raise ValueError(kind)
 
 
@@ -201,7 +206,7 @@ def mixed_mic_spline(device="cuda", instances=256, seed=4, mic_log2=(8, 18), spl
                     ctypes.byref(stream_h))
             req.tensors += [o_p, cache]
             out.append(Instance("spline", n, es, N, req, (fn, args), o_p, key.numel(),
-                                algorithmic_lookups("spline", N, n, bo, m, d)))
+                                algorithmic_lookups("spline", N, n, bo, m, d, tiling=True)))
         del s0, s1
     torch.cuda.synchronize(dev)
     return out

@@ -79,11 +79,22 @@ def test_spline_golden(F, name):
 @pytest.mark.parametrize("es,n,bo,m,d", [(8, 64, 64, 32, 2), (2, 16, 16, 7, 1), (4, 32, 24, 4, 5), (1, 8, 8, 3, 0),
                                          (8, 48, 64, 2, 8), (8, 40, 40, 5, 1), (8, 64, 56, 3, 3), (4, 32, 32, 2, 0),
                                          (2, 12, 12, 5, 2), (4, 32, 32, 9, 2), (8, 64, 64, 1, 0)])
-def test_spline_vs_oracle(F, oracle, es, n, bo, m, d):
-    rng = np.random.default_rng(zlib.crc32(repr(("spline", es, n, bo, m, d)).encode()))
+@pytest.mark.parametrize("layout", ["partition", "rotated", "gaps"])
+def test_spline_vs_oracle(F, oracle, es, n, bo, m, d, layout):
+    """Intervals that tile the ring (a partition from 0, or one rotated so that an interval
+    wraps) take the shared-endpoint walks; intervals with gaps take one walk per endpoint."""
+    rng = np.random.default_rng(zlib.crc32(repr(("spline", es, n, bo, m, d, layout)).encode()))
     N = 40
     a, s0, s1 = rnd(rng, N, es, n), seeds(rng, N), seeds(rng, N)
-    L, R = sorted_partition(rng, m, es, n)
+    if layout == "gaps":
+        L, R = random_intervals(rng, m, es, n)
+    else:
+        L, R = sorted_partition(rng, m, es, n)
+        if layout == "rotated":
+            r = int(rnd(rng, 1, 8, n)[0])
+            mask = (1 << n) - 1
+            L = np.array([(int(v) + r) & mask for v in L], dtype=np.uint64).astype(L.dtype)
+            R = np.array([(int(v) + r) & mask for v in R], dtype=np.uint64).astype(R.dtype)
     c = rnd(rng, m * (d + 1), es, 8 * es)
     kref, eref, bref = oracle.spline_keygen(a, s0, s1, c, d, L, R, n, bo)
     key, e, beta = empty_bytes(), empty_ring(es), empty_ring(es)
