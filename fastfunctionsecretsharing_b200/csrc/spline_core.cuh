@@ -78,14 +78,19 @@ __device__ __forceinline__ void slot_counters(uint32_t W[2][NB][4], const uint32
 // Adds the shares of values j0 .. j0 + cnt - 1 read out of the windows W[k] (the encrypted
 // slot blocks of convert stream k, or for a stream that needs no AES its key block itself in
 // W[k][0]) into acc[k][c], with the correction corr[j0 + c] where tc[k] is set.
-template <typename GE, int NB>
-__device__ __forceinline__ void slot_accumulate(const uint32_t W[2][NB][4], const uint32_t tc[2], const GE *corr,
-                                                uint32_t party, uint32_t ges, uint32_t off, uint32_t j0,
-                                                uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+template <typename GE>
+__device__ __forceinline__ void load_corr(uint64_t cv[kSplineMaxC], const GE *corr, uint32_t j0, uint32_t cnt)
 {
-    uint64_t cv[kSplineMaxC];
 #pragma unroll
     for (int c = 0; c < kSplineMaxC; c++) cv[c] = ((uint32_t)c < cnt) ? (uint64_t)__ldg(corr + j0 + c) : 0;
+}
+
+// cv: the corrections corr[j0 + c], loaded by the caller ahead of the AES work (load_corr)
+template <int NB>
+__device__ __forceinline__ void slot_accumulate(const uint32_t W[2][NB][4], const uint32_t tc[2],
+                                                const uint64_t cv[kSplineMaxC], uint32_t party, uint32_t ges,
+                                                uint32_t off, uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+{
 #pragma unroll
     for (int k = 0; k < 2; k++)
     {
@@ -179,6 +184,8 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
             prg_block(st[k][0], 2 * dir[k]);
             prg_block(st[k][1], 2 * dir[k] + 1);
         }
+        uint64_t cv[kSplineMaxC];
+        load_corr<GE>(cv, K.vCW + (size_t)lv * g, j0, cnt); // consumed after the AES work
         if (AES)
         {
             slot_counters<NB>(W, ctr);
@@ -194,12 +201,15 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
                 for (int c = 0; c < 4; c++) W[k][0][c] = v[k][c];
             }
         }
-        slot_accumulate<GE, NB>(W, tp, K.vCW + (size_t)lv * g, party, ges, off, j0, cnt, acc);
+        slot_accumulate<NB>(W, tp, cv, party, ges, off, cnt, acc);
         tp[0] = t[0], tp[1] = t[1];
         walk_advance(s, t, v, st, dir, cw, K.tl, K.tr, l1);
     }
     // level n - 1's convert and the leaf convert (keyed by the final seeds) together
     uint32_t W[2][NB][4], WL[2][NB][4];
+    uint64_t cv[kSplineMaxC], cl[kSplineMaxC];
+    load_corr<GE>(cv, K.vCW + (size_t)(n - 1) * g, j0, cnt);
+    load_corr<GE>(cl, K.last, j0, cnt);
     if (AES)
     {
         slot_counters<NB>(W, ctr);
@@ -215,17 +225,17 @@ __device__ __forceinline__ void spline_walk_pair(const AesLanes &A, const DcfKey
             for (int c = 0; c < 4; c++) W[k][0][c] = v[k][c], WL[k][0][c] = s[k][c];
         }
     }
-    slot_accumulate<GE, NB>(W, tp, K.vCW + (size_t)(n - 1) * g, party, ges, off, j0, cnt, acc);
-    slot_accumulate<GE, NB>(WL, t, K.last, party, ges, off, j0, cnt, acc);
+    slot_accumulate<NB>(W, tp, cv, party, ges, off, cnt, acc);
+    slot_accumulate<NB>(WL, t, cl, party, ges, off, cnt, acc);
 }
 
 // As slot_accumulate for two windows of ONE convert stream: window w is blocks
 // [w NB, w NB + NB) of W (a stream that needs no AES: its key block W[0] for both), read at byte
-// offset off[w] for values j0[w] .. j0[w] + cnt - 1, into acc[w][c].
-template <typename GE, int NB, bool AES>
-__device__ __forceinline__ void slot_accumulate2(const uint32_t W[][4], uint32_t tc, const GE *corr, uint32_t party,
-                                                 uint32_t ges, const uint32_t off[2], const uint32_t j0[2],
-                                                 uint32_t cnt, uint64_t acc[2][kSplineMaxC])
+// offset off[w], into acc[w][c], with the corrections cv[w][c] where tc is set.
+template <int NB, bool AES>
+__device__ __forceinline__ void slot_accumulate2(const uint32_t W[][4], uint32_t tc, const uint64_t cv[2][kSplineMaxC],
+                                                 uint32_t party, uint32_t ges, const uint32_t off[2], uint32_t cnt,
+                                                 uint64_t acc[2][kSplineMaxC])
 {
 #pragma unroll
     for (int w = 0; w < 2; w++)
@@ -237,8 +247,7 @@ __device__ __forceinline__ void slot_accumulate2(const uint32_t W[][4], uint32_t
         {
             if ((uint32_t)c < cnt)
             {
-                const uint64_t val = window_value<NB>(D, off[w] + (uint32_t)c * ges, ges) +
-                                     (tc ? (uint64_t)__ldg(corr + j0[w] + c) : 0);
+                const uint64_t val = window_value<NB>(D, off[w] + (uint32_t)c * ges, ges) + (tc ? cv[w][c] : 0);
                 acc[w][c] += party ? (0 - val) : val;
             }
         }
@@ -320,6 +329,9 @@ __device__ __forceinline__ void spline_walk_shared(const AesLanes &A, const DcfK
         uint32_t       st[1][2][4], W[1][WB][4];
         prg_block(st[0][0], 2 * dir);
         prg_block(st[0][1], 2 * dir + 1);
+        uint64_t cv[2][kSplineMaxC];
+        load_corr<GE>(cv[0], K.vCW + (size_t)lv * g, j0a, cnt); // consumed after the AES work
+        load_corr<GE>(cv[1], K.vCW + (size_t)lv * g, j0b, cnt);
         if (AES)
         {
             counters(W[0]);
@@ -331,12 +343,17 @@ __device__ __forceinline__ void spline_walk_shared(const AesLanes &A, const DcfK
 #pragma unroll
             for (int c = 0; c < 4; c++) W[0][0][c] = v[0][c];
         }
-        slot_accumulate2<GE, NB, AES>(W[0], tp, K.vCW + (size_t)lv * g, party, ges, off, j0, cnt, acc);
+        slot_accumulate2<NB, AES>(W[0], tp, cv, party, ges, off, cnt, acc);
         tp = t;
         advance(st, dir, cw, l1);
     }
     // level n - 1's convert and the leaf convert (keyed by the final seed) together
     uint32_t W[2][WB][4];
+    uint64_t cv[2][kSplineMaxC], cl[2][kSplineMaxC];
+    load_corr<GE>(cv[0], K.vCW + (size_t)(n - 1) * g, j0a, cnt);
+    load_corr<GE>(cv[1], K.vCW + (size_t)(n - 1) * g, j0b, cnt);
+    load_corr<GE>(cl[0], K.last, j0a, cnt);
+    load_corr<GE>(cl[1], K.last, j0b, cnt);
     if (AES)
     {
         counters(W[0]);
@@ -349,8 +366,8 @@ __device__ __forceinline__ void spline_walk_shared(const AesLanes &A, const DcfK
 #pragma unroll
         for (int c = 0; c < 4; c++) W[0][0][c] = v[0][c], W[1][0][c] = s[0][c];
     }
-    slot_accumulate2<GE, NB, AES>(W[0], tp, K.vCW + (size_t)(n - 1) * g, party, ges, off, j0, cnt, acc);
-    slot_accumulate2<GE, NB, AES>(W[1], t, K.last, party, ges, off, j0, cnt, acc);
+    slot_accumulate2<NB, AES>(W[0], tp, cv, party, ges, off, cnt, acc);
+    slot_accumulate2<NB, AES>(W[1], t, cl, party, ges, off, cnt, acc);
 }
 
 // The group sums w_c += cx beta_qc - s_qc + s'_qc + e_qc are reduced with shuffles and lane 0
