@@ -28,83 +28,11 @@ struct DcfKeyView
     }
 };
 
-// One level of the evaluation walk: expands the child on direction `dir` of node (s, t)
-// (blocks 2 dir and 2 dir + 1 of G(s)), applies the correction word, and leaves the
-// child's seed in s, its control bit in the return value and its value block in v.
-__device__ __forceinline__ uint32_t dcf_step(const AesLanes &A, uint32_t s[4], uint32_t t, uint32_t dir,
-                                             const uint8_t *cwp, uint64_t tl, uint64_t tr, uint32_t lv, uint32_t v[4])
-{
-    uint32_t cw[4];
-    load_block_be(cwp, cw);
-    uint32_t st[2][4];
-    {
-        const uint32_t sk[1][4] = {{s[0], s[1], s[2], s[3]}}, d1[1] = {dir};
-        uint32_t       sn[1][4], vv[1][4];
-        aes_prg_pair<1, 4>(A, sk, d1, sn, vv);
-#pragma unroll
-        for (int c = 0; c < 4; c++) st[0][c] = sn[0][c], st[1][c] = vv[0][c];
-    }
-    uint32_t       tn = (st[0][0] >> 24) & 1u;
-    const uint32_t m  = 0u - t;
-    st[0][0] &= ~kSeedTBit;
-#pragma unroll
-    for (int c = 0; c < 4; c++)
-    {
-        s[c] = st[0][c] ^ (cw[c] & m);
-        v[c] = st[1][c];
-    }
-    tn ^= (uint32_t)(((dir ? tr : tl) >> lv) & 1u) & t;
-    return tn;
-}
-
-// Share of output value `j` only (the group is read out of the convert stream without
-// materialising the other values): used where a caller consumes a slice of the group.
-// out[k] += share of value j0 + k, k < cnt (cnt <= MAXC).
-template <typename GE, int MAXC>
-__device__ __forceinline__ void dcf_eval_slice(const AesLanes &A, uint64_t out[MAXC], const DcfKeyView<GE> &K,
-                                               const uint8_t *seed, uint32_t party, uint32_t n, uint32_t bo,
-                                               uint32_t g, uint64_t x, uint32_t j0, uint32_t cnt)
-{
-    uint32_t s[4];
-    load_block_be(seed, s);
-    s[0] &= ~kSeedTBit;
-    uint32_t t = party;
-#pragma unroll 1
-    for (uint32_t lv = 0; lv < n; lv++)
-    {
-        const uint32_t dir = (uint32_t)((x >> (n - 1 - lv)) & 1u);
-        uint32_t       v[4];
-        const uint32_t tp = t;
-        t                 = dcf_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv, v);
-        ConvertStream cv;
-        cv.init(v, g, bo);
-#pragma unroll
-        for (int k = 0; k < MAXC; k++)
-        {
-            if ((uint32_t)k < cnt)
-            {
-                const uint64_t val = cv.value(A, j0 + k) + (tp ? (uint64_t)__ldg(K.vCW + (size_t)lv * g + j0 + k) : 0);
-                out[k] += party ? (0 - val) : val;
-            }
-        }
-    }
-    ConvertStream cv;
-    cv.init(s, g, bo);
-#pragma unroll
-    for (int k = 0; k < MAXC; k++)
-    {
-        if ((uint32_t)k < cnt)
-        {
-            const uint64_t val = cv.value(A, j0 + k) + (t ? (uint64_t)__ldg(K.last + j0 + k) : 0);
-            out[k] += party ? (0 - val) : val;
-        }
-    }
-}
-
-// One level for groupSize 1 of NK walks under the same key (correction words shared): like
-// dcf_step, but each value child is produced only as far as its first VW words (the bytes a
-// groupSize-1 convert reads: ceil(bo / 8) <= 4 VW).
-// The correction word cw[] (big-endian words) is supplied by the caller.
+// One level for groupSize 1 of NK walks under the same key (correction words shared): expands
+// the child on direction dir[k] of node (s[k], t[k]) — blocks 2 dir and 2 dir + 1 of G(s) — and
+// applies the correction word cw[] (big-endian words, supplied by the caller) where t is set.
+// The value child is produced only as far as its first VW words (the bytes a groupSize-1
+// convert reads: ceil(bo / 8) <= 4 VW).
 template <int NK, int VW>
 __device__ __forceinline__ void dcf_step_g1_cw(const AesLanes &A, uint32_t s[NK][4], uint32_t t[NK],
                                                const uint32_t dir[NK], const uint32_t cw[4], uint64_t tl, uint64_t tr,

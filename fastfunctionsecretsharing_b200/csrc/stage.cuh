@@ -1,5 +1,5 @@
-// stage.cuh — bulk asynchronous global -> shared copies completed on a shared-memory mbarrier
-// (sm_90+ `cp.async.bulk` and `mbarrier` PTX), used to stage per-warp key data. Every wait is
+// stage.cuh — asynchronous (TMA) global -> shared copies completed on a shared-memory mbarrier
+// (sm_90+ `cp.async.bulk.tensor` and `mbarrier` PTX), used to stage per-warp key data. Every wait is
 // bounded: after about a second the caller gets `false` and must record the timeout and stop
 // using the stage.
 #pragma once
@@ -69,15 +69,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
         if (global_ns() - t0 > kStageWaitNs) return false;
     }
     return false;
-}
-
-// `bytes` (a multiple of 16) from 16-byte aligned global `src` to 16-byte aligned shared
-// `dst`, completing on `bar`. No multicast.
-__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
 }
 
 // One box of a 2-D tiled tensor map (`map`: generic address of a __grid_constant__ CUtensorMap)
