@@ -20,7 +20,7 @@ import torch
 from . import _lib
 
 __all__ = [
-    "mod", "dtype",
+    "mod", "dtype", "logical_shape", "logical_numel",
     "dcf_get_key_data_size", "dcf_key_gen", "dcf_eval",
     "dpf_get_key_data_size", "dpf_key_gen", "dpf_eval", "dpf_eval_all", "dpf_multi_eval",
     "grotto_get_key_data_size", "grotto_key_gen", "grotto_eq_eval", "grotto_eval", "grotto_mic_eval",
@@ -56,6 +56,31 @@ def dtype(bit_width: int) -> torch.dtype:
     if bit_width <= 32:
         return torch.int32
     return torch.int64
+
+
+def _wide_limb_num(bit_width: int) -> int:
+    return 1 if bit_width <= 64 else (bit_width + 63) // 64
+
+
+def logical_shape(x: torch.Tensor, bit_width: int) -> torch.Size:
+    """Shape of the ring elements held by x (pyFastFss/__init__.py:52-61): x.shape up to 64 bits;
+    wider rings are int64 tensors whose last dimension holds the 64-bit limbs (the kernels of this
+    library evaluate rings of up to 64 bits)."""
+    if bit_width <= 64:
+        return x.shape
+    if x.dtype != torch.int64:
+        raise ValueError("wideint tensors must use torch.int64 dtype")
+    if x.ndim < 1 or x.shape[-1] != _wide_limb_num(bit_width):
+        raise ValueError("wideint tensor last dimension must equal limb count")
+    return x.shape[:-1]
+
+
+def logical_numel(x: torch.Tensor, bit_width: int) -> int:
+    """Number of ring elements held by x (pyFastFss/__init__.py:63-72)."""
+    n = 1
+    for dim in logical_shape(x, bit_width):
+        n *= dim
+    return n
 
 
 def _nbytes(t: torch.Tensor | None) -> int:
@@ -434,14 +459,24 @@ def get_fine_grain_parallel_grid_dim_threshold() -> int:
 
 
 class Prng:
-    """AES-128-CTR generator on the GPU (FastFss_cuda_prng*)."""
+    """AES-128-CTR generator on the GPU (FastFss_cuda_prng*), with the method set of the
+    reference binding's ``pyFastFss.Prng`` (lib/torch_extension/pyFastFss/csrc/bind_prng.cpp:8-17,
+    pyFastPrng.cpp): ``device()``, ``set_current_seed(seed128bit, counter128bit)``,
+    ``get_current_seed()``, ``to_(device)``, ``rand_(out, bitWidth)``. CUDA devices only."""
 
     def __init__(self, device: torch.device | str = "cuda"):
-        self.device = torch.device(device)
-        with torch.cuda.device(self.device):
-            self._h = _lib.fn("FastFss_cuda_prngInit")()
-        if not self._h:
+        self._device = torch.device(device)
+        if self._device.type != "cuda":
+            raise ValueError("device not supported: FastFss-B200 runs on CUDA tensors only")
+        self._h = self._init(self._device)
+
+    @staticmethod
+    def _init(device: torch.device):
+        with torch.cuda.device(device):
+            h = _lib.fn("FastFss_cuda_prngInit")()
+        if not h:
             raise RuntimeError("FastFss_cuda_prngInit failed")
+        return h
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -449,18 +484,45 @@ class Prng:
             _lib.fn("FastFss_cuda_prngRelease")(h)
             self._h = None
 
-    def set_current_seed(self, seed: bytes, counter: bytes | None = None) -> None:
+    def device(self) -> torch.device:
+        return self._device
+
+    def set_current_seed(self, seed128bit: bytes, counter128bit: bytes) -> None:
+        if len(seed128bit) != 16 or len(counter128bit) != 16:
+            raise RuntimeError("seed128bit and counter128bit must be 16 bytes")
         _check("FastFss_cuda_prngSetCurrentSeed",
-               _lib.fn("FastFss_cuda_prngSetCurrentSeed")(self._h, seed, counter))
+               _lib.fn("FastFss_cuda_prngSetCurrentSeed")(self._h, bytes(seed128bit), bytes(counter128bit)))
 
     def get_current_seed(self) -> tuple[bytes, bytes]:
         s, c = ctypes.create_string_buffer(16), ctypes.create_string_buffer(16)
         _check("FastFss_cuda_prngGetCurrentSeed", _lib.fn("FastFss_cuda_prngGetCurrentSeed")(self._h, s, c))
         return s.raw, c.raw
 
-    def gen(self, out: torch.Tensor, bitWidth: int) -> torch.Tensor:
-        dev = _cuda(out)
-        st = _Stream(dev)
+    def to_(self, device: torch.device | str) -> "Prng":
+        """Moves the generator (seed and counter) to another CUDA device."""
+        device = torch.device(device)
+        if device.type != "cuda":
+            raise ValueError("device not supported: FastFss-B200 runs on CUDA tensors only")
+        seed, counter = self.get_current_seed()
+        h = self._init(device)
+        with torch.cuda.device(device):
+            rc = _lib.fn("FastFss_cuda_prngSetCurrentSeed")(h, seed, counter)
+        if rc != 0:
+            _lib.fn("FastFss_cuda_prngRelease")(h)
+            raise RuntimeError("FastFss_prngSetCurrentSeed failed")
+        _lib.fn("FastFss_cuda_prngRelease")(self._h)
+        self._h, self._device = h, device
+        return self
+
+    def rand_(self, out: torch.Tensor, bitWidth: int) -> torch.Tensor:
+        """Fills `out` (values reduced to bitWidth bits) from the stream and returns it."""
+        if not out.is_contiguous():
+            raise ValueError("assert fail: out.is_contiguous()")
+        if out.device.type != self._device.type:
+            raise ValueError("assert fail: device_.type() == out.device().type()")
+        if bitWidth > out.element_size() * 8:
+            raise ValueError("assert fail: bitWidth <= elementSize * 8")
+        st = _Stream(out.device)
         _check("FastFss_cuda_prngGen", _lib.fn("FastFss_cuda_prngGen")(
             self._h, _ptr(out), bitWidth, out.element_size(), out.numel(), st.ptr))
         return out

@@ -148,17 +148,23 @@ def test_prng_golden_and_counter(F, oracle):
     P = F.Prng("cuda")
     P.set_current_seed(g["seed"].tobytes(), g["counter"].tobytes())
     out = torch.empty(g["out"].size, dtype=torch.uint8, device="cuda")
-    P.gen(out, 8)
+    assert P.rand_(out, 8) is out
     assert np.array_equal(host(out), g["out"])
     assert P.get_current_seed()[1] == g["counter_after"].tobytes()
     # a second call continues the stream exactly like the CPU generator
     out2 = torch.empty(333, dtype=torch.uint8, device="cuda")
-    P.gen(out2, 8)
+    P.rand_(out2, 8)
     want, ctr = oracle.prng(g["seed"].tobytes(), g["counter_after"].tobytes(), 333)
     assert np.array_equal(host(out2), want) and P.get_current_seed()[1] == ctr
     # unaligned destination
     buf = torch.zeros(1000, dtype=torch.uint8, device="cuda")
-    P.set_current_seed(bytes(16))
-    P.gen(buf[3:3 + 500], 8)
+    P.set_current_seed(bytes(16), bytes(16))
+    P.rand_(buf[3:3 + 500], 8)
     want, _ = oracle.prng(bytes(16), bytes(16), 500)
     assert np.array_equal(host(buf[3:503]), want) and not host(buf[:3]).any()
+    # the reference binding's contract: 16-byte seed and counter, device() and to_()
+    assert P.device() == torch.device("cuda")
+    with pytest.raises(RuntimeError, match="16 bytes"):
+        P.set_current_seed(bytes(8), bytes(16))
+    before = P.get_current_seed()
+    assert P.to_(torch.device("cuda", 0)) is P and P.get_current_seed() == before
