@@ -40,7 +40,9 @@ struct BatchOpDev
 };
 
 constexpr size_t kBatchHeader    = 256; // tile counter, then padding
-constexpr int    kBatchSmemExtra = 16;  // broadcast slot for the claimed tile
+// after the tables: the claimed tile (16 B), then the MIC point shares (one per thread, 512 at
+// most) and their count
+constexpr int    kBatchSmemExtra = 16 + 512 * 8 + 16;
 
 template <typename GE>
 __device__ __forceinline__ void batch_run_tile(const AesLanes &A, const BatchOpDev &op, unsigned long long first,
@@ -71,10 +73,29 @@ __device__ __forceinline__ void batch_run_tile(const AesLanes &A, const BatchOpD
             }
             break;
         case FAST_FSS_BATCH_DCF_MIC_EVAL:
-            for (unsigned long long k = first + threadIdx.x; k < last; k += blockDim.x)
-                out[k] = mic_eval_item<GE>(A, xs, key, (const GE *)op.aux0, seed, party, (const GE *)op.L,
-                                           (const GE *)op.R, op.m, n, bo, N, k);
+        {
+            // touching intervals: the elements the tile's items belong to, each point walked
+            // once (mic_shared_batch); otherwise one item per thread, both walks
+            uint64_t *shares = reinterpret_cast<uint64_t *>(fss_smem + kAesSmemTotal + 16);
+            uint32_t *points = reinterpret_cast<uint32_t *>(shares + blockDim.x);
+            if (threadIdx.x == 0) *points = mic_points<GE>((const GE *)op.L, (const GE *)op.R, op.m, n);
+            __syncthreads();
+            const uint32_t P = *points;
+            if (P != 0 && P <= blockDim.x)
+            {
+                const size_t e0 = first / op.m, e1 = (last + op.m - 1) / op.m, E = blockDim.x / P;
+                for (size_t base = e0; base < e1; base += E)
+                    mic_shared_batch<GE>(A, shares, out, xs, key, (const GE *)op.aux0, seed, party, (const GE *)op.L,
+                                         (const GE *)op.R, op.m, n, bo, N, P, base, e1, first, last);
+            }
+            else
+            {
+                for (unsigned long long k = first + threadIdx.x; k < last; k += blockDim.x)
+                    out[k] = mic_eval_item<GE>(A, xs, key, (const GE *)op.aux0, seed, party, (const GE *)op.L,
+                                               (const GE *)op.R, op.m, n, bo, N, k);
+            }
             break;
+        }
         case FAST_FSS_BATCH_SPLINE_EVAL:
         {
             // whole warps iterate together (the group reduction shuffles)

@@ -4,10 +4,11 @@
 // (validation), include/FastFss/cuda/mic.h (ABI). The key is a DCF key with groupSize 1
 // for alpha - 1 and beta = 1; z[i][q] is public per-interval correction data.
 //
-// Evaluation runs one thread per (element, interval): both DCF walks of the interval,
-// sp = DCF(x - 1 - L_q) and sq = DCF(x - 1 - (R_q + 1)). (The reference walks each element's
-// intervals on one thread and reuses sq of interval q - 1 as sp of interval q when they
-// touch; both are evaluations at the same point, so shares are identical.)
+// Evaluation: interval q needs sp = DCF(x - 1 - L_q) and sq = DCF(x - 1 - (R_q + 1)). When the
+// intervals touch, sq of interval q - 1 is sp of interval q (the reference reuses it in its
+// per-element loop); here each point is walked once by its own thread and the intervals are
+// formed from neighbouring points after a barrier. Intervals that do not touch are evaluated
+// one thread per (element, interval), both walks side by side.
 #include <FastFss/cuda/mic.h>
 #include <FastFss/mic.h>
 
@@ -51,6 +52,11 @@ __global__ void __launch_bounds__(kMicThreads, 1)
     }
 }
 
+// Touching intervals share endpoint walks, as the reference's own loop does when it reuses sq
+// of interval q - 1 as sp of interval q (src/impl/mic.h:60-105): a CTA takes E = blockDim / P
+// elements at a time, thread t walks point t % P of element t / P into shared memory, and after
+// a barrier thread t writes interval t % m of element t / m from the two points around it.
+// Otherwise one thread per (element, interval) walks both endpoints (mic_eval_item).
 template <typename GE>
 __global__ void __launch_bounds__(kMicThreads, 1)
     mic_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
@@ -59,11 +65,24 @@ __global__ void __launch_bounds__(kMicThreads, 1)
                     size_t N)
 {
     aes_tables_build();
-    AesLanes     A;
-    const size_t work = N * m;
+    AesLanes A;
     A.init();
-    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
-        out[w] = mic_eval_item<GE>(A, maskedX, key, z, seed, party, left, right, m, n, bo, N, w);
+    uint64_t *shares = reinterpret_cast<uint64_t *>(fss_smem + kAesSmemTotal); // blockDim entries
+    uint32_t *points = reinterpret_cast<uint32_t *>(shares + blockDim.x);
+    if (threadIdx.x == 0) *points = mic_points<GE>(left, right, m, n);
+    __syncthreads();
+    const uint32_t P = *points;
+    if (P == 0 || P > blockDim.x)
+    {
+        const size_t work = N * m;
+        for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+            out[w] = mic_eval_item<GE>(A, maskedX, key, z, seed, party, left, right, m, n, bo, N, w);
+        return;
+    }
+    const uint32_t E = blockDim.x / P;
+    for (size_t base = (size_t)blockIdx.x * E; base < N; base += (size_t)gridDim.x * E)
+        mic_shared_batch<GE>(A, shares, out, maskedX, key, z, seed, party, left, right, m, n, bo, N, P, base, N, 0,
+                             (unsigned long long)N * m);
 }
 
 static inline size_t dcf_key_bytes_g1(size_t n, size_t es, size_t N)
@@ -135,9 +154,11 @@ extern "C" FAST_FSS_API int FastFss_cuda_dcfMICEval(void *sharedOut, size_t shar
         if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
         if (int rc = check_alignment(es, {sharedOut, maskedX, sharedZ, leftEndpoints, rightEndpoints}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
         auto kern = mic_eval_kernel<GE>;
-        if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
-        kern<<<grid_for(N * m, aes_threads(N * m, kMicThreads), 1), aes_threads(N * m, kMicThreads), kAesSmemTotal,
-                 resolve_stream(cudaStreamPtr)>>>(
+        // tables, then one share per thread and the point count (mic_eval_kernel)
+        constexpr int smem = kAesSmemTotal + kMicThreads * 8 + 16;
+        if (!ensure_smem(reinterpret_cast<const void *>(kern), smem)) return FAST_FSS_RUNTIME_ERROR;
+        const int threads = aes_threads(N * m, kMicThreads);
+        kern<<<grid_for(N * m, threads, 1), threads, kAesSmemTotal + threads * 8 + 16, resolve_stream(cudaStreamPtr)>>>(
             (GE *)sharedOut, (const GE *)maskedX, (const uint8_t *)key, (const GE *)sharedZ, (const uint8_t *)seed,
             (uint32_t)partyId, (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)n,
             (uint32_t)bitWidthOut, N);

@@ -96,7 +96,8 @@ def spline_window_blocks(m: int, cn: int, c0: int, cnt: int, ges: int) -> int:
 def algorithmic_lookups(kind: str, N: int, n: int, bo: int, m: int = 0, d: int = 0, tiling: bool = False) -> int:
     """AES table lookups one party's evaluation needs.
 
-    mic: 2 m groupSize-1 DCF walks of n levels per element.
+    mic: 2 m groupSize-1 DCF walks of n levels per element; with `tiling` (here: touching
+    intervals, R_q + 1 = L_{q+1}) each of the m + 1 endpoint points is walked once.
     spline: per element and interval, two DCF walks of n levels; a level is the node expansion
     (key schedule + seed child + full value child, 346) and the convert of interval q's d + 1
     values out of the value child's AES-CTR stream (key schedule + the blocks holding them);
@@ -105,7 +106,8 @@ def algorithmic_lookups(kind: str, N: int, n: int, bo: int, m: int = 0, d: int =
     right endpoint of interval q - 1: one walk per interval, whose converts read two slot
     windows (slots q and q - 1) under one key schedule."""
     if kind == "mic":
-        return N * m * 2 * n * dcf_level_lookups(bo)
+        walks = (m + 1) if tiling else 2 * m
+        return N * walks * n * dcf_level_lookups(bo)
     if kind == "spline":
         cn, ges = d + 1, (bo + 7) // 8
         g = m * cn
@@ -179,7 +181,7 @@ def mixed_mic_spline(device="cuda", instances=256, seed=4, mic_log2=(8, 18), spl
                     Rt.data_ptr(), Rt.numel() * es, n, bo, es, N, None, 0, ctypes.byref(stream_h))
             req.tensors += [o_p]
             out.append(Instance("mic", n, es, N, req, (fn, args), o_p, key.numel(),
-                                algorithmic_lookups("mic", N, n, bo, mic_intervals)))
+                                algorithmic_lookups("mic", N, n, bo, mic_intervals, tiling=True)))
         else:
             m, d = spline_intervals, degree
             L, R = partition(rng, m, n)

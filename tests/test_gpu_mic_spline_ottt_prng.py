@@ -42,12 +42,35 @@ def test_mic_golden(F, name):
         assert np.array_equal(host(out, es), g[f"y{p}"])
 
 
-@pytest.mark.parametrize("es,n,bo,m", [(1, 8, 8, 3), (2, 15, 16, 9), (4, 32, 32, 16), (8, 64, 64, 16), (8, 40, 17, 5)])
-def test_mic_vs_oracle(F, oracle, es, n, bo, m):
-    rng = np.random.default_rng(zlib.crc32(repr(("dmic", es, n, bo, m)).encode()))
+def touching_intervals(rng, m, es, n):
+    """m intervals [b_q, b_{q+1} - 1] between sorted distinct boundaries (they touch, but the
+    last does not wrap round to the first)."""
+    dom = 1 << n
+    b = set()
+    while len(b) < m + 1:
+        b.add(int(rnd(rng, 1, 8, n)[0]) % dom)
+    b = sorted(b)
+    L = np.array(b[:-1], dtype=np.uint64).astype(DTYPES[es])
+    R = np.array([(v - 1) % dom for v in b[1:]], dtype=np.uint64).astype(DTYPES[es])
+    return L, R
+
+
+@pytest.mark.parametrize("es,n,bo,m", [(1, 8, 8, 3), (2, 15, 16, 9), (4, 32, 32, 16), (8, 64, 64, 16), (8, 40, 17, 5),
+                                       (4, 20, 32, 40), (2, 16, 16, 1)])
+@pytest.mark.parametrize("layout", ["random", "touching", "tiling"])
+def test_mic_vs_oracle(F, oracle, es, n, bo, m, layout):
+    """Touching intervals (each point walked once and shared by the two intervals around it;
+    tiling: the last also touches the first) and independent intervals (two walks per
+    interval) give the oracle's shares."""
+    rng = np.random.default_rng(zlib.crc32(repr(("dmic", es, n, bo, m, layout)).encode()))
     N = 257
     a, s0, s1 = rnd(rng, N, es, n), seeds(rng, N), seeds(rng, N)
-    L, R = random_intervals(rng, m, es, n)
+    if layout == "random":
+        L, R = random_intervals(rng, m, es, n)
+    elif layout == "touching":
+        L, R = touching_intervals(rng, m, es, n)
+    else:
+        L, R = sorted_partition(rng, m, es, n)
     kref, zref = oracle.dcf_mic_keygen(a, s0, s1, L, R, n, bo)
     key, z = empty_bytes(), empty_ring(es)
     F.dcf_mic_key_gen(key, z, dev_ring(a), dev_bytes(s0), dev_bytes(s1), dev_ring(L), dev_ring(R), n, bo)
