@@ -139,6 +139,119 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
     }
 }
 
+// MIC and interval LUT by endpoint points walked once each. Interval q needs the comparison
+// shares at xP_q = x - (L_q - 1) and xQ_q = x - R_q. When the intervals touch (R_q + 1 =
+// L_{q+1}), xQ_q is xP_{q+1} (the reference reuses it the same way, src/impl/grotto.h:414-423):
+// the m + 1 points xP_0 .. xP_{m-1}, xQ_{m-1} serve all m intervals, or m points when the last
+// interval also touches the first; otherwise each interval has its own 2 points. A CTA takes E
+// elements at a time: their points are walked two per thread (both walks in the same AES
+// calls, grotto_cmp2) into shared-memory bytes, and after a barrier each output (MIC: one interval's bit; LUT: E or one T_j, summed over the
+// intervals) is formed from the bytes. Shares equal grotto_interval_bit's.
+constexpr uint32_t kPointBytes = 32768; // shared-memory bytes for point shares per CTA pass
+
+template <typename GE>
+__device__ __forceinline__ uint32_t grotto_points_layout(const GE *left, const GE *right, uint32_t m, uint32_t n)
+{
+    // 0: independent intervals (2 m points); 1: touching chain (m + 1); 2: touching cycle (m)
+    for (uint32_t q = 0; q + 1 < m; q++)
+        if (mod_bits<GE>((uint64_t)(GE)((uint64_t)__ldg(left + q + 1) - 1), n) != mod_bits<GE>((uint64_t)__ldg(right + q), n))
+            return 0;
+    return mod_bits<GE>((uint64_t)(GE)((uint64_t)__ldg(left) - 1), n) == mod_bits<GE>((uint64_t)__ldg(right + m - 1), n)
+               ? 2
+               : 1;
+}
+
+// Point p of an element with masked input mx under the given layout.
+template <typename GE>
+__device__ __forceinline__ uint64_t grotto_point(const GE *left, const GE *right, uint32_t m, uint32_t n,
+                                                 uint32_t layout, uint64_t mx, uint32_t p)
+{
+    uint32_t q;
+    bool     isQ;
+    if (layout == 0)
+        q = p >> 1, isQ = (p & 1u) != 0;
+    else
+        q = p < m ? p : m - 1, isQ = p == m;
+    const uint64_t e = isQ ? (uint64_t)__ldg(right + q) : (uint64_t)(GE)((uint64_t)__ldg(left + q) - 1);
+    return mod_bits<GE>((uint64_t)(GE)(mx - e), n);
+}
+
+template <typename GE, bool LUT>
+__global__ void __launch_bounds__(kGrottoThreads, 1)
+    grotto_intervals_kernel(GE *__restrict__ out, GE *__restrict__ outT, const GE *__restrict__ maskedX,
+                            const uint8_t *__restrict__ key, const uint8_t *__restrict__ seed, uint32_t party,
+                            const GE *__restrict__ left, const GE *__restrict__ right, const GE *__restrict__ lut,
+                            uint32_t lutNum, uint32_t m, uint32_t n, size_t N)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    uint32_t *layoutSlot = reinterpret_cast<uint32_t *>(fss_smem + kAesSmemTotal);
+    uint8_t  *bits       = fss_smem + kAesSmemTotal + 16;
+    if (threadIdx.x == 0) *layoutSlot = grotto_points_layout<GE>(left, right, m, n);
+    __syncthreads();
+    const uint32_t layout = *layoutSlot;
+    const uint32_t P      = layout == 0 ? 2 * m : (layout == 1 ? m + 1 : m);
+    const uint32_t H      = (P + 1) / 2; // point pairs per element: one thread walks two points
+    uint32_t       E      = blockDim.x / H;
+    E                     = E < 1 ? 1 : E;
+    if (E * P > kPointBytes) E = kPointBytes / P; // the host keeps 2 m <= kPointBytes
+    if (E == 0) return;
+    const uint32_t outs = LUT ? 1 + lutNum : m;     // outputs per element
+    for (size_t base = (size_t)blockIdx.x * E; base < N; base += (size_t)gridDim.x * E)
+    {
+        for (uint32_t idx = threadIdx.x; idx < E * H; idx += blockDim.x)
+        {
+            const size_t i = base + idx / H;
+            if (i >= N) continue;
+            GrottoKeyView<GE> K;
+            K.set(key, n, i, N);
+            const uint32_t e = idx / H, p0 = 2 * (idx % H), p1 = p0 + 1 < P ? p0 + 1 : p0;
+            const uint64_t mx    = (uint64_t)__ldg(maskedX + i);
+            const uint64_t pt[2] = {grotto_point<GE>(left, right, m, n, layout, mx, p0),
+                                    grotto_point<GE>(left, right, m, n, layout, mx, p1)};
+            uint32_t       sh[2];
+            grotto_cmp2<GE>(A, K, seed + 16 * i, party, n, pt, true, sh);
+            bits[e * P + p0] = (uint8_t)sh[0];
+            bits[e * P + p1] = (uint8_t)sh[1];
+        }
+        __syncthreads();
+        for (uint32_t idx = threadIdx.x; idx < E * outs; idx += blockDim.x)
+        {
+            const size_t i = base + idx / outs;
+            if (i >= N) continue;
+            const uint32_t e = idx / outs, o = idx % outs;
+            const uint64_t mx = (uint64_t)__ldg(maskedX + i);
+            // interval q's bit from its two points (layout as grotto_point)
+            auto bit = [&](uint32_t q) -> uint32_t {
+                const uint32_t a = layout == 0 ? 2 * q : q;
+                const uint32_t b = layout == 0 ? 2 * q + 1 : (q + 1 == P ? 0 : q + 1);
+                // point b is xQ_q itself, or (touching) xP_{q+1} = xQ_q
+                const uint64_t xP = grotto_point<GE>(left, right, m, n, layout, mx, a);
+                const uint64_t xQ = grotto_point<GE>(left, right, m, n, layout, mx, b);
+                return (bits[e * P + a] ^ bits[e * P + b] ^ ((xQ >= xP) ? party : 0u)) & 1u;
+            };
+            if (!LUT)
+            {
+                out[i * m + o] = (GE)bit(o);
+                continue;
+            }
+            uint64_t acc = 0;
+            for (uint32_t q = 0; q < m; q++)
+            {
+                const uint64_t b = bit(q);
+                acc += (o == 0) ? b : b * (uint64_t)__ldg(lut + q + (size_t)(o - 1) * m);
+            }
+            if (party) acc = 0 - acc;
+            if (o == 0)
+                out[i] = (GE)acc;
+            else
+                outT[i * lutNum + (o - 1)] = (GE)acc;
+        }
+        __syncthreads();
+    }
+}
+
 // Interval LUT (src/impl/grotto.h:449-545): G lanes per element stride over the intervals;
 // E and T[j0 .. j0 + LMAX) are summed in the ring and reduced with warp shuffles.
 template <typename GE, int LMAX>
@@ -382,6 +495,17 @@ static int launch(K kern, size_t work, cudaStream_t stream, Args... args)
     return launch_status();
 }
 
+template <typename GE, bool LUT, typename... Args>
+static int launch_intervals(size_t N, size_t m, cudaStream_t stream, Args... args)
+{
+    auto          kern = grotto_intervals_kernel<GE, LUT>;
+    constexpr int smem = kAesSmemTotal + 16 + (int)kPointBytes;
+    if (!ensure_smem(reinterpret_cast<const void *>(kern), smem)) return FAST_FSS_RUNTIME_ERROR;
+    const int threads = aes_threads(N * m, kGrottoThreads);
+    kern<<<grid_for(N * m, threads, 1), threads, smem, stream>>>(args...);
+    return launch_status();
+}
+
 } // namespace fss
 
 using namespace fss;
@@ -491,6 +615,11 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoMICEval(void *sharedBooleanOut, s
             return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0 || m == 0) return FAST_FSS_SUCCESS;
         if (int rc = check_alignment(es, {sharedBooleanOut, maskedX, leftEndpoints, rightEndpoints}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
+        if (2 * m <= kPointBytes)
+            return launch_intervals<GE, false>(N, m, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut, nullptr,
+                                               (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed,
+                                               (uint32_t)partyId, (const GE *)leftEndpoints,
+                                               (const GE *)rightEndpoints, nullptr, 0u, (uint32_t)m, (uint32_t)n, N);
         return launch(grotto_mic_kernel<GE>, N * m, resolve_stream(cudaStreamPtr), (GE *)sharedBooleanOut,
                       (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
                       (const GE *)leftEndpoints, (const GE *)rightEndpoints, (uint32_t)m, (uint32_t)n, N);
@@ -527,9 +656,14 @@ extern "C" FAST_FSS_API int FastFss_cuda_grottoIntervalLutEval(
             return FAST_FSS_INVALID_CACHE_DATA_SIZE_ERROR;
         if (N == 0) return FAST_FSS_SUCCESS;
         if (int rc = check_alignment(es, {sharedOutE, sharedOutT, maskedX, leftEndpoints, rightEndpoints, lookUpTable}, {key, seed}); rc != FAST_FSS_SUCCESS) return rc;
+        cudaStream_t stream = resolve_stream(cudaStreamPtr);
+        if (2 * m <= kPointBytes)
+            return launch_intervals<GE, true>(N, m, stream, (GE *)sharedOutE, (GE *)sharedOutT, (const GE *)maskedX,
+                                              (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+                                              (const GE *)leftEndpoints, (const GE *)rightEndpoints,
+                                              (const GE *)lookUpTable, (uint32_t)lutNum, (uint32_t)m, (uint32_t)n, N);
         uint32_t G = 1;
         while (G < 32 && G < m) G <<= 1;
-        cudaStream_t stream = resolve_stream(cudaStreamPtr);
         constexpr int LMAX = 4;
         for (size_t j0 = 0; j0 < (lutNum ? lutNum : 1); j0 += LMAX)
         {

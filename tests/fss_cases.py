@@ -46,6 +46,19 @@ def random_intervals(rng, m: int, es: int, n: int):
     return np.minimum(a, b).astype(DTYPES[es]), np.maximum(a, b).astype(DTYPES[es])
 
 
+def touching_intervals(rng, m: int, es: int, n: int):
+    """m intervals [b_q, b_{q+1} - 1] between sorted distinct boundaries (each touches the next,
+    but the last does not wrap round to the first)."""
+    dom = 1 << n
+    b: set[int] = set()
+    while len(b) < m + 1:
+        b.add(int(rnd(rng, 1, 8, n)[0]) % dom)
+    bs = sorted(b)
+    L = np.array(bs[:-1], dtype=np.uint64).astype(DTYPES[es])
+    R = np.array([(v - 1) % dom for v in bs[1:]], dtype=np.uint64).astype(DTYPES[es])
+    return L, R
+
+
 def take_elements(key: np.ndarray, regions: list[int], N: int, idx: np.ndarray) -> np.ndarray:
     """Rebuilds a key buffer holding elements `idx` of a key whose layout is a sequence of
     element-major regions with the given per-element byte strides."""

@@ -7,7 +7,7 @@ import zlib
 import numpy as np
 import pytest
 from conftest import golden_names, load_golden
-from fss_cases import random_intervals, rnd, seeds, sorted_partition
+from fss_cases import random_intervals, rnd, seeds, sorted_partition, touching_intervals
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -80,16 +80,24 @@ def test_grid_vs_oracle(F, oracle, es, n):
             assert np.array_equal(point(F, "cmp", x, key, s, p, n, eb), oracle.grotto_eval(x, kref, s, eb, p, n))
 
 
-@pytest.mark.parametrize("es,n,m,lutn", [(2, 16, 64, 1), (1, 8, 5, 3), (4, 20, 33, 6), (8, 64, 7, 2)])
-@pytest.mark.parametrize("partition", [True, False])
-def test_mic_lut_vs_oracle(F, oracle, es, n, m, lutn, partition):
-    rng = np.random.default_rng(zlib.crc32(repr(("mic", es, n, m, partition)).encode()))
+@pytest.mark.parametrize("es,n,m,lutn", [(2, 16, 64, 1), (1, 8, 5, 3), (4, 20, 33, 6), (8, 64, 7, 2), (2, 12, 1, 2),
+                                        (4, 24, 300, 9)])
+@pytest.mark.parametrize("layout", ["partition", "touching", "random"])
+def test_mic_lut_vs_oracle(F, oracle, es, n, m, lutn, layout):
+    """Partitions (touching, the last round to the first), touching chains and independent
+    intervals: each endpoint point walked once where intervals share it."""
+    rng = np.random.default_rng(zlib.crc32(repr(("mic", es, n, m, layout)).encode()))
     N = 300
     a, s0, s1 = rnd(rng, N, es, n), seeds(rng, N), seeds(rng, N)
     kref = oracle.grotto_keygen(a, s0, s1, n)
     key = dev_bytes(kref)
     x = rnd(rng, N, es, 8 * es)
-    L, R = sorted_partition(rng, m, es, n) if partition else random_intervals(rng, m, es, n)
+    if layout == "partition":
+        L, R = sorted_partition(rng, m, es, n)
+    elif layout == "touching":
+        L, R = touching_intervals(rng, m, es, n)
+    else:
+        L, R = random_intervals(rng, m, es, n)
     lut = rnd(rng, m * lutn, es, 8 * es)
     for p, s in ((0, s0), (1, s1)):
         out = empty_ring(es)

@@ -6,7 +6,7 @@ import zlib
 import numpy as np
 import pytest
 from conftest import golden_names, load_golden
-from fss_cases import DTYPES, random_intervals, rnd, seeds, sorted_partition
+from fss_cases import DTYPES, random_intervals, rnd, seeds, sorted_partition, touching_intervals
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -40,19 +40,6 @@ def test_mic_golden(F, name):
         F.dcf_mic_eval(out, dev_ring(g["maskedX"]), key, dev_ring(g[f"z{p}"]), dev_bytes(g[f"seed{p}"]), p,
                        dev_ring(g["left"]), dev_ring(g["right"]), g["n"], g["bo"])
         assert np.array_equal(host(out, es), g[f"y{p}"])
-
-
-def touching_intervals(rng, m, es, n):
-    """m intervals [b_q, b_{q+1} - 1] between sorted distinct boundaries (they touch, but the
-    last does not wrap round to the first)."""
-    dom = 1 << n
-    b = set()
-    while len(b) < m + 1:
-        b.add(int(rnd(rng, 1, 8, n)[0]) % dom)
-    b = sorted(b)
-    L = np.array(b[:-1], dtype=np.uint64).astype(DTYPES[es])
-    R = np.array([(v - 1) % dom for v in b[1:]], dtype=np.uint64).astype(DTYPES[es])
-    return L, R
 
 
 @pytest.mark.parametrize("es,n,bo,m", [(1, 8, 8, 3), (2, 15, 16, 9), (4, 32, 32, 16), (8, 64, 64, 16), (8, 40, 17, 5),
