@@ -67,6 +67,8 @@ class Request:
     done: float = 0.0
     x_host: torch.Tensor | None = None
     out_host: torch.Tensor | None = None
+    x_dev: torch.Tensor | None = None    # the request's device buffers, allocated before serving
+    out_dev: torch.Tensor | None = None  # starts (nothing is allocated while requests are served)
 
 
 @dataclass
@@ -171,7 +173,9 @@ def mlp_trace(rng: np.random.Generator, layers=12, width=4096, batch_rows=64, lo
 
 def make_requests(P: Pools, rate: float, count: int, seed: int = 1, dcf_log2=(10, 20), spline_log2=(10, 14)):
     """`count` requests of the MLP trace with Poisson arrivals at `rate` per second (arrival
-    times relative to the start). Host inputs and outputs are pinned."""
+    times relative to the start). Host inputs and outputs are pinned; each request's device
+    input and output buffers are allocated here too, so that serving itself allocates nothing
+    (an allocation that has to free cached device memory synchronises the whole device)."""
     rng = np.random.default_rng(seed)
     trace = mlp_trace(rng, lo=dcf_log2[0], hi=dcf_log2[1], spline_hi=spline_log2[1], limit=count)
     t = 0.0
@@ -186,7 +190,10 @@ def make_requests(P: Pools, rate: float, count: int, seed: int = 1, dcf_log2=(10
             xb = torch.from_numpy(rng.integers(-2**63, 2**63 - 1, size=size, dtype=np.int64)).pin_memory()
             ob = torch.empty(size, dtype=torch.int64).pin_memory()
             kb = size * SPLINE_KEY_BYTES
-        out.append(Request(rid, kind, layer, size, t, kb, x_host=xb, out_host=ob))
+        dt = torch.int32 if kind == "dcf" else torch.int64
+        out.append(Request(rid, kind, layer, size, t, kb, x_host=xb, out_host=ob,
+                           x_dev=torch.empty(size, dtype=dt, device=P.dev),
+                           out_dev=torch.empty(size, dtype=dt, device=P.dev)))
     return out
 
 
@@ -221,7 +228,9 @@ class Server:
             for n in pool:
                 dt = torch.int32 if kind == "dcf" else torch.int64
                 reqs.append(Request(-1, kind, 0, n, 0.0, 0, x_host=torch.zeros(n, dtype=dt).pin_memory(),
-                                    out_host=torch.empty(n, dtype=dt).pin_memory()))
+                                    out_host=torch.empty(n, dtype=dt).pin_memory(),
+                                    x_dev=torch.empty(n, dtype=dt, device=self.dev),
+                                    out_dev=torch.empty(n, dtype=dt, device=self.dev)))
         s = self.slots[0]
         with torch.cuda.stream(s):
             for r in reqs:
@@ -235,14 +244,12 @@ class Server:
         P = self.P
         if r.kind == "dcf":
             c = P.dcf[r.size]
-            x = torch.empty(r.size, dtype=torch.int32, device=self.dev)
+            x, out = r.x_dev, r.out_dev
             x.copy_(r.x_host, non_blocking=True)
-            out = torch.empty(0, dtype=torch.int32, device=self.dev)
             return batch.dcf_request(out, x, c.key, c.seed, P.party, DCF_N, DCF_N)
         c = P.spline[r.size]
-        x = torch.empty(r.size, dtype=torch.int64, device=self.dev)
+        x, out = r.x_dev, r.out_dev
         x.copy_(r.x_host, non_blocking=True)
-        out = torch.empty(0, dtype=torch.int64, device=self.dev)
         return batch.spline_request(out, x, c.key, c.e, c.beta, c.seed, P.party, P.spline_L, P.spline_R, SPLINE_M,
                                     SPLINE_D, SPLINE_N, SPLINE_N)
 
@@ -252,9 +259,8 @@ class Server:
         h = ctypes.c_void_p(stream.cuda_stream)
         if r.kind == "dcf":
             c = P.dcf[r.size]
-            x = torch.empty(r.size, dtype=torch.int32, device=self.dev)
+            x, out = r.x_dev, r.out_dev
             x.copy_(r.x_host, non_blocking=True)
-            out = torch.empty(r.size, dtype=torch.int32, device=self.dev)
             rc = _lib.fn("FastFss_cuda_dcfEval")(out.data_ptr(), 4 * r.size, x.data_ptr(), 4 * r.size,
                                                 c.key.data_ptr(), c.key.numel(), c.seed.data_ptr(), 16 * r.size,
                                                 P.party, DCF_N, DCF_N, 1, 4, r.size, None, 0, ctypes.byref(h))
@@ -262,9 +268,8 @@ class Server:
         else:
             c = P.spline[r.size]
             g = SPLINE_G
-            x = torch.empty(r.size, dtype=torch.int64, device=self.dev)
+            x, out = r.x_dev, r.out_dev
             x.copy_(r.x_host, non_blocking=True)
-            out = torch.empty(r.size, dtype=torch.int64, device=self.dev)
             cache = c.cache
             csize = cache.numel()
             rc = _lib.fn("FastFss_cuda_dcfSplineEval")(
@@ -275,7 +280,7 @@ class Server:
             keep = (x, out, cache)
         if rc != 0:
             raise RuntimeError(f"plain evaluation failed : {rc}")
-        r.out_host.copy_(out, non_blocking=True)
+        r.out_host.copy_(out.view(-1), non_blocking=True)
         return keep
 
     def run(self, requests: list[Request], mode: str = "batched", poll_s: float = 2e-5) -> float:
