@@ -493,12 +493,57 @@ def dpf_section(dev, args, peak_glookups) -> dict:
     del alpha, beta, s0, s1, x, masked, key, y0, y1
     torch.cuda.empty_cache()
     ach = DPF_LOOKUPS_PER_ELEM * N / (ms / 1e3) / 1e9
+    full = dpf_all_section(dev, args, peak_glookups)
     return {"workload": "plain DPF eval, 2^24 elements, n=32, Z_2^32 (uint32), groupSize 1, one party per step",
             "elements": N, "kernel_ms": ms, "value": N / (ms / 1e3) / 1e9, "unit": "Gelem/s",
             "aes_blocks_per_s": (N_BITS + 1) * N / (ms / 1e3), "key_bytes_per_element": key_bytes / N,
             "hbm_gbs": (key_bytes + N * (16 + 4 + 4)) / (ms / 1e3) / 1e9,
             "roofline": {"bound": "smem", "achieved": ach, "peak": peak_glookups, "unit": "Glookup/s",
                          "frac": ach / peak_glookups, "algorithmic_lookups_per_element": DPF_LOOKUPS_PER_ELEM},
+            "shares_reconstruct": ok, "eval_all": full}
+
+
+# Full-domain DPF per key at n = 16, groupSize 1, 32-bit output: 2^n - 1 node expansions of
+# both children under one key schedule (40 + 18 shared first-round + 2 x 144 rounds 2-9 and
+# last = 346 lookups) and 2^n leaf converts (40 + 148, as above).
+DPF_ALL_N = 16
+DPF_ALL_LOOKUPS_PER_KEY = ((1 << DPF_ALL_N) - 1) * 346 + (1 << DPF_ALL_N) * (40 + 148)
+
+
+def dpf_all_section(dev, args, peak_glookups) -> dict:
+    """Full-domain DPF evaluation (FastFss_cuda_dpfEvalAll): 2^12 keys at n = 16 over Z_2^32
+    (uint32), groupSize 1, every key expanded to its 2^16 outputs (1 GiB of shares per party)."""
+    import torch
+
+    import fastfunctionsecretsharing_b200 as F
+
+    n, N = DPF_ALL_N, 1 << 12
+    gen = torch.Generator(device=dev).manual_seed(8765)
+    alpha = torch.randint(0, 1 << n, (N,), dtype=torch.int32, device=dev, generator=gen)
+    beta = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
+    s0 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    s1 = torch.randint(0, 256, (N * 16,), dtype=torch.uint8, device=dev, generator=gen)
+    x = torch.randint(0, 1 << n, (N,), dtype=torch.int32, device=dev, generator=gen)
+    masked = (x + alpha) & ((1 << n) - 1)
+    key = torch.empty(0, dtype=torch.uint8, device=dev)
+    F.dpf_key_gen(key, alpha, beta, s0, s1, n, 32, 1)
+    y0 = torch.empty(0, dtype=torch.int32, device=dev)
+    y1 = torch.empty(0, dtype=torch.int32, device=dev)
+    ms = _timed(lambda: F.dpf_eval_all(y0, masked, key, s0, 0, n, 32, 1), dev, max(3, min(args.steps, 10)))
+    F.dpf_eval_all(y1, masked, key, s1, 1, n, 32, 1)
+    # out[i][(maskedX - j) mod 2^n] = share of beta [j == alpha]: the reconstruction holds beta at x
+    want = torch.zeros(N, 1 << n, dtype=torch.int32, device=dev)
+    want[torch.arange(N, device=dev), x.long()] = beta
+    ok = bool(torch.equal((y0 + y1).view(N, 1 << n), want))
+    out_bytes = y0.numel() * 4
+    del alpha, beta, s0, s1, x, masked, key, y0, y1, want
+    torch.cuda.empty_cache()
+    ach = DPF_ALL_LOOKUPS_PER_KEY * N / (ms / 1e3) / 1e9
+    return {"workload": "full-domain DPF eval, 2^12 keys, n=16, Z_2^32 (uint32), groupSize 1, one party per step",
+            "keys": N, "kernel_ms": ms, "Gout_per_s": N * (1 << n) / (ms / 1e3) / 1e9,
+            "out_gbs": out_bytes / (ms / 1e3) / 1e9,
+            "roofline": {"bound": "smem", "achieved": ach, "peak": peak_glookups, "unit": "Glookup/s",
+                         "frac": ach / peak_glookups, "algorithmic_lookups_per_key": DPF_ALL_LOOKUPS_PER_KEY},
             "shares_reconstruct": ok}
 
 

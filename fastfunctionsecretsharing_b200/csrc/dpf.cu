@@ -91,12 +91,13 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     }
 }
 
-// mode 1: evalAll (work = N 2^n); mode 2: evalMulti (N P). Plain eval is dpf_eval_staged_kernel.
-template <typename GE, int MODE>
+// Multi-point evaluation (work = N P): point j of element i evaluates at maskedX - point[j]
+// (src/kernel/dpf.h:490-495), one tree walk per (element, point).
+template <typename GE>
 __global__ void __launch_bounds__(kDpfThreads, 1)
-    dpf_eval_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
-                    const uint8_t *__restrict__ seed, const GE *__restrict__ point, uint32_t party, uint32_t n,
-                    uint32_t bo, uint32_t g, size_t N, size_t per, size_t work)
+    dpf_eval_multi_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                          const uint8_t *__restrict__ seed, const GE *__restrict__ point, uint32_t party, uint32_t n,
+                          uint32_t bo, uint32_t g, size_t N, size_t per, size_t work)
 {
     aes_tables_build();
     AesLanes A;
@@ -104,32 +105,97 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     const size_t bstr = sizeof(GE) * (2 + (size_t)g);
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
     {
-        const size_t i  = (MODE == 0) ? w : w / per;
-        const size_t j  = (MODE == 0) ? 0 : w % per;
-        const GE    *kb = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
-        uint64_t     x;
-        GE          *o;
-        if (MODE == 0)
+        const size_t   i  = w / per, j = w % per;
+        const GE      *kb = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
+        const uint64_t x  = mod_bits<GE>((uint64_t)(GE)((uint64_t)__ldg(maskedX + i) - (uint64_t)__ldg(point + j)), n);
+        dpf_eval_point<GE>(A, out + (i * per + j) * g, key + i * 16 * n, kb, seed + 16 * i, party, n, bo, g, x,
+                           (uint64_t)__ldg(kb), (uint64_t)__ldg(kb + 1));
+    }
+}
+
+// Full-domain evaluation: out[i][(maskedX - x) mod 2^n] = dpfEval(x) for every x < 2^n
+// (src/kernel/dpf.h:268-275). A thread owns one subtree of 2^d leaves of one element: it
+// walks the n - d levels above the subtree root along the subtree index, then expands the
+// subtree depth first, computing both children of a node under one key schedule
+// (aes_prg_children) and keeping the corrected right siblings on a stack. An element costs
+// 2^n - 1 node expansions plus 2^n leaf converts instead of n 2^n single-child steps.
+constexpr uint32_t kDpfAllMaxSub = 7;
+
+template <typename GE>
+__global__ void __launch_bounds__(kDpfThreads, 1)
+    dpf_eval_all_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
+                        const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, uint32_t bo, uint32_t g,
+                        size_t N, uint32_t d)
+{
+    aes_tables_build();
+    AesLanes A;
+    A.init();
+    const uint32_t top   = n - d;
+    const size_t   S     = (size_t)1 << top;
+    const size_t   work  = N * S;
+    const size_t   per   = (size_t)1 << n;
+    const size_t   nleaf = (size_t)1 << d;
+    const size_t   bstr  = sizeof(GE) * (2 + (size_t)g);
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t   i    = w >> top, sub = w & (S - 1);
+        const uint8_t *sCWp = key + i * 16 * n;
+        const GE      *kb   = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
+        const uint64_t tl = (uint64_t)__ldg(kb), tr = (uint64_t)__ldg(kb + 1);
+        const size_t   mx = (size_t)__ldg(maskedX + i);
+        uint32_t       s[4];
+        load_block_be(seed + 16 * i, s);
+        s[0] &= ~kSeedTBit;
+        uint32_t t = party;
+#pragma unroll 1
+        for (uint32_t lv = 0; lv < top; lv++)
         {
-            x = (uint64_t)__ldg(maskedX + i);
-            o = out + i * g;
+            uint32_t cw[4];
+            load_block_be(sCWp + 16 * lv, cw);
+            t = dpf_step(A, s, t, (uint32_t)((sub >> (top - 1 - lv)) & 1u), cw, tl, tr, lv);
         }
-        else if (MODE == 1)
+        // right-sibling stack: seed words and control bit per depth below the subtree root
+        uint32_t     stk[kDpfAllMaxSub][5];
+        uint32_t     depth = 0;
+        const size_t x0    = sub << d;
+#pragma unroll 1
+        for (size_t j = 0; j < nleaf; j++)
         {
-            // src/kernel/dpf.h:268-275: out index (maskedX - x) mod 2^n holds dpfEval(x).
-            x                   = (uint64_t)j;
-            const size_t target = ((size_t)__ldg(maskedX + i) - j) & (per - 1);
-            o                   = out + (i * per + target) * g;
+#pragma unroll 1
+            while (depth < d)
+            {
+                const uint32_t lv = top + depth;
+                uint32_t       cw[4], st[2][4];
+                load_block_be(sCWp + 16 * lv, cw);
+                aes_prg_children<0xF>(A, s, st[0], st[1]);
+                const uint32_t m  = 0u - t;
+                uint32_t       tL = (st[0][0] >> 24) & 1u, tR = (st[1][0] >> 24) & 1u;
+                st[0][0] &= ~kSeedTBit;
+                st[1][0] &= ~kSeedTBit;
+                tL ^= (uint32_t)((tl >> lv) & 1u) & t;
+                tR ^= (uint32_t)((tr >> lv) & 1u) & t;
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+                {
+                    stk[depth][c] = st[1][c] ^ (cw[c] & m);
+                    s[c]          = st[0][c] ^ (cw[c] & m);
+                }
+                stk[depth][4] = tR;
+                t             = tL;
+                depth++;
+            }
+            dpf_leaf<GE>(A, out + (i * per + ((mx - (x0 + j)) & (per - 1))) * g, s, t, kb, party, bo, g);
+            if (j + 1 < nleaf)
+            {
+                // next leaf: the right sibling at depth d - 1 - ctz(j + 1)
+                const uint32_t p = (uint32_t)__ffsll((long long)(j + 1)) - 1;
+                depth            = d - 1 - p;
+#pragma unroll
+                for (int c = 0; c < 4; c++) s[c] = stk[depth][c];
+                t = stk[depth][4];
+                depth++;
+            }
         }
-        else
-        {
-            // src/kernel/dpf.h:490-495: point j evaluates at maskedX - point[j] (ring).
-            x = (uint64_t)(GE)((uint64_t)__ldg(maskedX + i) - (uint64_t)__ldg(point + j));
-            o = out + (i * per + j) * g;
-        }
-        x = mod_bits<GE>(x, n);
-        dpf_eval_point<GE>(A, o, key + i * 16 * n, kb, seed + 16 * i, party, n, bo, g, x, (uint64_t)__ldg(kb),
-                           (uint64_t)__ldg(kb + 1));
     }
 }
 
@@ -247,9 +313,21 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
             (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, map);
         return launch_status();
     }
+    else if constexpr (MODE == 1)
+    {
+        const uint32_t d       = n < kDpfAllMaxSub ? (uint32_t)n : kDpfAllMaxSub;
+        const size_t   units   = N << (n - d);
+        auto           kern    = dpf_eval_all_kernel<GE>;
+        if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
+        const int threads = aes_threads(units, kDpfThreads);
+        kern<<<grid_for(units, threads, 1), threads, kAesSmemTotal, stream>>>(
+            (GE *)out, (const GE *)maskedX, (const uint8_t *)key, (const uint8_t *)seed, (uint32_t)partyId,
+            (uint32_t)n, (uint32_t)bo, (uint32_t)g, N, d);
+        return launch_status();
+    }
     else
     {
-        auto kern = dpf_eval_kernel<GE, MODE>;
+        auto kern = dpf_eval_multi_kernel<GE>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
         const int threads = aes_threads(work, kDpfThreads);
         kern<<<grid_for(work, threads, 1), threads, kAesSmemTotal, stream>>>(

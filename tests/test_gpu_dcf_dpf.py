@@ -112,8 +112,11 @@ def test_dpf_eval_all_and_multi_golden(F):
         assert np.array_equal(host(out, 2), g[f"y{p}"])
 
 
-@pytest.mark.parametrize("es,n,g", [(1, 8, 1), (2, 10, 3), (4, 12, 1), (8, 9, 2)])
+@pytest.mark.parametrize("es,n,g", [(1, 8, 1), (2, 10, 3), (4, 12, 1), (8, 9, 2), (1, 1, 1), (1, 3, 2), (2, 6, 1),
+                                    (4, 7, 1), (8, 5, 17), (4, 14, 1), (2, 16, 1)])
 def test_dpf_eval_all_multi_vs_oracle(F, oracle, es, n, g):
+    """Full domain: depth-first subtrees of up to 2^7 leaves under a walked prefix (n > 7), a
+    single subtree per element (n <= 7); multi-value leaves through the AES-CTR convert (g = 17)."""
     rng = np.random.default_rng(es * 100 + n)
     N, bo = 9, 8 * es
     a, b, s0, s1 = rnd(rng, N, es, n), rnd(rng, N * g, es, bo), seeds(rng, N), seeds(rng, N)
