@@ -117,11 +117,53 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
 // (src/kernel/dpf.h:268-275). A thread owns one subtree of 2^d leaves of one element: it
 // walks the n - d levels above the subtree root along the subtree index, then expands the
 // subtree depth first, computing both children of a node under one key schedule
-// (aes_prg_children) and keeping the corrected right siblings on a stack. An element costs
+// (aes_prg_children). Leaf parents emit both leaves at once; above them the corrected right
+// children wait on a stack (16-byte entries, control bits in a register). An element costs
 // 2^n - 1 node expansions plus 2^n leaf converts instead of n 2^n single-child steps.
-constexpr uint32_t kDpfAllMaxSub = 7;
+constexpr uint32_t kDpfAllMaxSub = 8;
 
-template <typename GE>
+// Both children of the node (s, t) at level lv, corrected by cw when t is set.
+__device__ __forceinline__ void dpf_children(const AesLanes &A, const uint32_t s[4], uint32_t t, const uint32_t cw[4],
+                                             uint64_t tl, uint64_t tr, uint32_t lv, uint32_t L[4], uint32_t &tL,
+                                             uint32_t R[4], uint32_t &tR)
+{
+    aes_prg_children<0xF>(A, s, L, R);
+    const uint32_t m = 0u - t;
+    tL               = ((L[0] >> 24) & 1u) ^ ((uint32_t)((tl >> lv) & 1u) & t);
+    tR               = ((R[0] >> 24) & 1u) ^ ((uint32_t)((tr >> lv) & 1u) & t);
+    L[0] &= ~kSeedTBit;
+    R[0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+    {
+        L[c] ^= cw[c] & m;
+        R[c] ^= cw[c] & m;
+    }
+}
+
+// One leaf's g outputs. With groupSize 1 (G1) the convert (init(seed, bitWidthOut, 1), values
+// of one byte) yields byte 0 of its stream: byte 0 of the seed when bitWidthOut <= 16, else
+// byte 0 of AES_seed(0^128).
+template <typename GE, bool G1>
+__device__ __forceinline__ void dpf_all_leaf(const AesLanes &A, GE *o, const uint32_t s[4], uint32_t t, const GE *kb,
+                                             uint64_t last, uint32_t party, uint32_t bo, uint32_t g)
+{
+    if constexpr (G1)
+    {
+        const uint32_t b = (bo <= 16) ? (s[0] >> 24) : (aes_zero_block_word0(A, s) >> 24);
+        const uint64_t v = (uint64_t)b + (t ? last : 0);
+        o[0]             = (GE)(party ? (0 - v) : v);
+    }
+    else
+    {
+        dpf_leaf<GE>(A, o, s, t, kb, party, bo, g);
+    }
+}
+
+// The loop has a single call site for the node expansion and one for the leaf convert, so
+// the kernel's code stays small; the n - d levels above the subtree also expand both
+// children and keep the one on the path.
+template <typename GE, bool G1>
 __global__ void __launch_bounds__(kDpfThreads, 1)
     dpf_eval_all_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
                         const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, uint32_t bo, uint32_t g,
@@ -134,67 +176,68 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     const size_t   S     = (size_t)1 << top;
     const size_t   work  = N * S;
     const size_t   per   = (size_t)1 << n;
-    const size_t   nleaf = (size_t)1 << d;
+    const size_t   npair = (size_t)1 << (d - 1); // leaf parents per subtree (d >= 1)
     const size_t   bstr  = sizeof(GE) * (2 + (size_t)g);
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
     {
         const size_t   i    = w >> top, sub = w & (S - 1);
         const uint8_t *sCWp = key + i * 16 * n;
         const GE      *kb   = reinterpret_cast<const GE *>(key + N * 16 * n + i * bstr);
-        const uint64_t tl = (uint64_t)__ldg(kb), tr = (uint64_t)__ldg(kb + 1);
+        const uint64_t tl = (uint64_t)__ldg(kb), tr = (uint64_t)__ldg(kb + 1), last = (uint64_t)__ldg(kb + 2);
         const size_t   mx = (size_t)__ldg(maskedX + i);
+        GE            *row = out + i * per * g;
         uint32_t       s[4];
         load_block_be(seed + 16 * i, s);
         s[0] &= ~kSeedTBit;
-        uint32_t t = party;
+        uint32_t     t = party;
+        uint4        stk[kDpfAllMaxSub - 1]; // right children below the subtree root (index: parent depth)
+        uint32_t     tstk = 0;
+        uint32_t     lv   = 0; // level of the node (s, t)
+        size_t       q    = 0; // leaf parents done
+        const size_t x0   = sub << d;
 #pragma unroll 1
-        for (uint32_t lv = 0; lv < top; lv++)
+        for (;;)
         {
-            uint32_t cw[4];
+            uint32_t cw[4], L[4], R[4], tL, tR;
             load_block_be(sCWp + 16 * lv, cw);
-            t = dpf_step(A, s, t, (uint32_t)((sub >> (top - 1 - lv)) & 1u), cw, tl, tr, lv);
-        }
-        // right-sibling stack: seed words and control bit per depth below the subtree root
-        uint32_t     stk[kDpfAllMaxSub][5];
-        uint32_t     depth = 0;
-        const size_t x0    = sub << d;
-#pragma unroll 1
-        for (size_t j = 0; j < nleaf; j++)
-        {
-#pragma unroll 1
-            while (depth < d)
+            dpf_children(A, s, t, cw, tl, tr, lv, L, tL, R, tR);
+            if (lv < top)
             {
-                const uint32_t lv = top + depth;
-                uint32_t       cw[4], st[2][4];
-                load_block_be(sCWp + 16 * lv, cw);
-                aes_prg_children<0xF>(A, s, st[0], st[1]);
-                const uint32_t m  = 0u - t;
-                uint32_t       tL = (st[0][0] >> 24) & 1u, tR = (st[1][0] >> 24) & 1u;
-                st[0][0] &= ~kSeedTBit;
-                st[1][0] &= ~kSeedTBit;
-                tL ^= (uint32_t)((tl >> lv) & 1u) & t;
-                tR ^= (uint32_t)((tr >> lv) & 1u) & t;
+                const bool right = (sub >> (top - 1 - lv)) & 1u;
 #pragma unroll
-                for (int c = 0; c < 4; c++)
-                {
-                    stk[depth][c] = st[1][c] ^ (cw[c] & m);
-                    s[c]          = st[0][c] ^ (cw[c] & m);
-                }
-                stk[depth][4] = tR;
-                t             = tL;
-                depth++;
+                for (int c = 0; c < 4; c++) s[c] = right ? R[c] : L[c];
+                t = right ? tR : tL;
+                lv++;
+                continue;
             }
-            dpf_leaf<GE>(A, out + (i * per + ((mx - (x0 + j)) & (per - 1))) * g, s, t, kb, party, bo, g);
-            if (j + 1 < nleaf)
+            const uint32_t depth = lv - top;
+            if (depth + 1 < d)
             {
-                // next leaf: the right sibling at depth d - 1 - ctz(j + 1)
-                const uint32_t p = (uint32_t)__ffsll((long long)(j + 1)) - 1;
-                depth            = d - 1 - p;
+                stk[depth] = make_uint4(R[0], R[1], R[2], R[3]);
+                tstk       = (tstk & ~(1u << depth)) | (tR << depth);
 #pragma unroll
-                for (int c = 0; c < 4; c++) s[c] = stk[depth][c];
-                t = stk[depth][4];
-                depth++;
+                for (int c = 0; c < 4; c++) s[c] = L[c];
+                t = tL;
+                lv++;
+                continue;
             }
+            const size_t x = x0 + 2 * q;
+#pragma unroll 1
+            for (uint32_t k = 0; k < 2; k++)
+            {
+                uint32_t ls[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) ls[c] = k ? R[c] : L[c];
+                dpf_all_leaf<GE, G1>(A, row + ((mx - x - k) & (per - 1)) * g, ls, k ? tR : tL, kb, last, party, bo,
+                                     g);
+            }
+            if (++q == npair) break;
+            // next leaf parent: the right child stacked at depth d - 2 - ctz(q)
+            const uint32_t dp = d - 2 - ((uint32_t)__ffsll((long long)q) - 1);
+            const uint4    e  = stk[dp];
+            s[0] = e.x, s[1] = e.y, s[2] = e.z, s[3] = e.w;
+            t  = (tstk >> dp) & 1u;
+            lv = top + dp + 1;
         }
     }
 }
@@ -317,7 +360,7 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
     {
         const uint32_t d       = n < kDpfAllMaxSub ? (uint32_t)n : kDpfAllMaxSub;
         const size_t   units   = N << (n - d);
-        auto           kern    = dpf_eval_all_kernel<GE>;
+        auto           kern    = (g == 1) ? dpf_eval_all_kernel<GE, true> : dpf_eval_all_kernel<GE, false>;
         if (!prepare_aes_kernel(kern)) return FAST_FSS_RUNTIME_ERROR;
         const int threads = aes_threads(units, kDpfThreads);
         kern<<<grid_for(units, threads, 1), threads, kAesSmemTotal, stream>>>(

@@ -190,6 +190,23 @@ __device__ __forceinline__ void aes_encrypt(const AesLanes& A, const uint32_t ke
     for (int b = 0; b < NB; b++) enc_last(A, st[b], w);
 }
 
+// Word 0 of AES_key(0^128). The state after the initial AddRoundKey of the all-zero block is
+// the key itself; the last round computes only the first column: 40 + 144 + 4 = 188 lookups.
+__device__ __forceinline__ uint32_t aes_zero_block_word0(const AesLanes& A, const uint32_t key[4])
+{
+    uint32_t           w[4]  = {key[0], key[1], key[2], key[3]};
+    uint32_t           st[4] = {key[0], key[1], key[2], key[3]};
+    constexpr uint32_t RCON[10] = {0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80, 0x1b, 0x36};
+#pragma unroll
+    for (int r = 0; r < 9; r++)
+    {
+        key_step(A, w, RCON[r]);
+        enc_round(A, st, w);
+    }
+    key_step(A, w, RCON[9]);
+    return sub_col(A, st[0], st[1], st[2], st[3]) ^ w[0];
+}
+
 // Blocks 2 dir and 2 dir + 1 of the GGM expansion under `key`: the seed child (all four words,
 // into sOut) and the value child (its first VW words, into vOut). Their plaintexts differ only
 // in bytes 0 and 8, which feed one lookup each of first-round columns 0 and 2, so the other 14
