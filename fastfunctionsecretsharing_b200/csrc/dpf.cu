@@ -122,25 +122,6 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
 // 2^n - 1 node expansions plus 2^n leaf converts instead of n 2^n single-child steps.
 constexpr uint32_t kDpfAllMaxSub = 8;
 
-// Both children of the node (s, t) at level lv, corrected by cw when t is set.
-__device__ __forceinline__ void dpf_children(const AesLanes &A, const uint32_t s[4], uint32_t t, const uint32_t cw[4],
-                                             uint64_t tl, uint64_t tr, uint32_t lv, uint32_t L[4], uint32_t &tL,
-                                             uint32_t R[4], uint32_t &tR)
-{
-    aes_prg_children<0xF>(A, s, L, R);
-    const uint32_t m = 0u - t;
-    tL               = ((L[0] >> 24) & 1u) ^ ((uint32_t)((tl >> lv) & 1u) & t);
-    tR               = ((R[0] >> 24) & 1u) ^ ((uint32_t)((tr >> lv) & 1u) & t);
-    L[0] &= ~kSeedTBit;
-    R[0] &= ~kSeedTBit;
-#pragma unroll
-    for (int c = 0; c < 4; c++)
-    {
-        L[c] ^= cw[c] & m;
-        R[c] ^= cw[c] & m;
-    }
-}
-
 // One leaf's g outputs. With groupSize 1 (G1) the convert (init(seed, bitWidthOut, 1), values
 // of one byte) yields byte 0 of its stream: byte 0 of the seed when bitWidthOut <= 16, else
 // byte 0 of AES_seed(0^128).
@@ -200,7 +181,7 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
         {
             uint32_t cw[4], L[4], R[4], tL, tR;
             load_block_be(sCWp + 16 * lv, cw);
-            dpf_children(A, s, t, cw, tl, tr, lv, L, tL, R, tR);
+            ggm_children(A, s, t, cw, tl, tr, lv, L, tL, R, tR);
             if (lv < top)
             {
                 const bool right = (sub >> (top - 1 - lv)) & 1u;

@@ -302,6 +302,27 @@ __device__ __forceinline__ void aes_prg_children(const AesLanes& A, const uint32
     }
 }
 
+// Both children of the tree node (s, t) at level lv, as evaluation derives them: the control
+// bit of a child is bit 0 of its byte 0 xor (its tCW bit at lv, i.e. bit lv of tl / tr) when
+// t is set; the seed is the child block with that bit cleared, xor cw when t is set.
+__device__ __forceinline__ void ggm_children(const AesLanes& A, const uint32_t s[4], uint32_t t, const uint32_t cw[4],
+                                             uint64_t tl, uint64_t tr, uint32_t lv, uint32_t L[4], uint32_t& tL,
+                                             uint32_t R[4], uint32_t& tR)
+{
+    aes_prg_children<0xF>(A, s, L, R);
+    const uint32_t m = 0u - t;
+    tL               = ((L[0] >> 24) & 1u) ^ ((uint32_t)((tl >> lv) & 1u) & t);
+    tR               = ((R[0] >> 24) & 1u) ^ ((uint32_t)((tr >> lv) & 1u) & t);
+    L[0] &= ~kSeedTBit;
+    R[0] &= ~kSeedTBit;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+    {
+        L[c] ^= cw[c] & m;
+        R[c] ^= cw[c] & m;
+    }
+}
+
 // Blocks 0..3 of the GGM expansion under `key` (block j: LE64(2j) || LE64(2j + 1)), as key
 // generation needs them: the seed children 0 and 2 in full, the value children 1 and 3 only as
 // far as their first VW words (VW = 4: in full). The four plaintexts differ only in bytes 0 and

@@ -333,6 +333,12 @@ __device__ __forceinline__ uint64_t excl_prefix_xor(uint64_t u)
     return p << 1;
 }
 
+// A thread owns a subtree of 2^d leaf words of one key: the n - 6 - d levels above it are
+// walked along the subtree index, then the subtree is expanded depth first. Every node
+// expansion (walk, interior and leaf parents) goes through the one ggm_children call site of
+// the loop, which keeps the kernel's code small; leaf parents emit both leaf words, and the
+// corrected right children wait on a stack of 16-byte entries whose control and parity bits
+// live in two registers.
 template <typename GE, int MODE> // MODE 0: equality rows, 1: comparison (equalBound) rows
 __global__ void __launch_bounds__(kGrottoThreads, 1)
     grotto_all_kernel(unsigned long long *__restrict__ out, const uint8_t *__restrict__ key,
@@ -346,74 +352,71 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
     const size_t   S     = (size_t)1 << top;
     const size_t   work  = N * S;
     const size_t   words = (size_t)1 << D; // leaf words per key
+    const size_t   nleaf = (size_t)1 << d;
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
     {
-        const size_t      i = w / S, sub = w % S;
+        const size_t      i = w >> top, sub = w & (S - 1);
         GrottoKeyView<GE> K;
         K.set(key, n, i, N);
         uint32_t s[4];
         load_block_be(seed + 16 * i, s);
         s[0] &= ~kSeedTBit;
-        uint32_t t = party, par = 0;
-        for (uint32_t lv = 0; lv < top; lv++)
+        uint32_t            t = party, par = 0;
+        unsigned long long *row = out + i * words + sub * nleaf;
+        // leaf word of seed x with control bit tx and right-turn parity px
+        auto leaf = [&](const uint32_t x[4], uint32_t tx, uint32_t px) -> unsigned long long {
+            const uint64_t u0 = hi_u64(x);
+            const uint64_t u  = tx ? (u0 ^ K.last) : u0;
+            return (MODE == 0) ? u : (excl_prefix_xor(u) ^ ((px ^ party) ? ~0ull : 0ull));
+        };
+        if (d == 0)
         {
-            const uint32_t dir = (uint32_t)((sub >> (top - 1 - lv)) & 1u);
-            const uint32_t tn  = grotto_step(A, s, t, dir, K.sCW + 16 * lv, K.tl, K.tr, lv);
-            par ^= dir & (t ^ tn);
-            t = tn;
+            row[0] = leaf(s, t, par); // n = 6: the root is the only leaf
+            continue;
         }
-        // right-sibling stack: seed words, control bit, parity per depth below the subtree root
-        uint32_t           stk[kAllMaxSub][6];
-        uint32_t           depth = 0;
-        const size_t       nleaf = (size_t)1 << d;
-        unsigned long long *row  = out + i * words + sub * nleaf;
-        for (size_t j = 0; j < nleaf; j++)
+        uint4    stk[kAllMaxSub - 1]; // right children below the subtree root (index: parent depth)
+        uint32_t tstk = 0, pstk = 0;
+        uint32_t lv = 0;               // level of the node (s, t)
+        size_t   q  = 0;               // leaf parents done
+#pragma unroll 1
+        for (;;)
         {
-            while (depth < d)
+            uint32_t cw[4], L[4], R[4], tL, tR;
+            load_block_be(K.sCW + 16 * lv, cw);
+            ggm_children(A, s, t, cw, K.tl, K.tr, lv, L, tL, R, tR);
+            if (lv < top)
             {
-                const uint32_t lv = top + depth;
-                uint32_t       cw[4];
-                load_block_be(K.sCW + 16 * lv, cw);
-                // leaf parents: a leaf reads words 2, 3 (its 64 bits) and word 0 (its control bit)
-                uint32_t st[2][4];
-                if (depth + 1 == d)
-                    aes_prg_children<0xD>(A, s, st[0], st[1]);
-                else
-                    aes_prg_children<0xF>(A, s, st[0], st[1]);
-                const uint32_t m  = 0u - t;
-                uint32_t       tL = (st[0][0] >> 24) & 1u, tR = (st[1][0] >> 24) & 1u;
-                st[0][0] &= ~kSeedTBit;
-                st[1][0] &= ~kSeedTBit;
-                tL ^= (uint32_t)((K.tl >> lv) & 1u) & t;
-                tR ^= (uint32_t)((K.tr >> lv) & 1u) & t;
+                const uint32_t dir = (uint32_t)((sub >> (top - 1 - lv)) & 1u);
+                const uint32_t tn  = dir ? tR : tL;
 #pragma unroll
-                for (int c = 0; c < 4; c++)
-                {
-                    stk[depth][c] = st[1][c] ^ (cw[c] & m);
-                    s[c]          = st[0][c] ^ (cw[c] & m);
-                }
-                stk[depth][4] = tR;
-                stk[depth][5] = par ^ (t ^ tR);
-                t             = tL;
-                depth++;
+                for (int c = 0; c < 4; c++) s[c] = dir ? R[c] : L[c];
+                par ^= dir & (t ^ tn);
+                t = tn;
+                lv++;
+                continue;
             }
-            const uint64_t u0 = hi_u64(s);
-            const uint64_t u  = t ? (u0 ^ K.last) : u0;
-            if (MODE == 0)
-                row[j] = u;
-            else
-                row[j] = excl_prefix_xor(u) ^ ((par ^ party) ? ~0ull : 0ull);
-            if (j + 1 < nleaf)
+            const uint32_t depth = lv - top;
+            if (depth + 1 < d)
             {
-                // next leaf: right sibling at depth d - 1 - ctz(j + 1)
-                const uint32_t p = (uint32_t)__ffsll((long long)(j + 1)) - 1;
-                depth            = d - 1 - p;
+                stk[depth] = make_uint4(R[0], R[1], R[2], R[3]);
+                tstk       = (tstk & ~(1u << depth)) | (tR << depth);
+                pstk       = (pstk & ~(1u << depth)) | ((par ^ t ^ tR) << depth);
 #pragma unroll
-                for (int c = 0; c < 4; c++) s[c] = stk[depth][c];
-                t   = stk[depth][4];
-                par = stk[depth][5];
-                depth++;
+                for (int c = 0; c < 4; c++) s[c] = L[c];
+                t = tL;
+                lv++;
+                continue;
             }
+            row[2 * q]     = leaf(L, tL, par);
+            row[2 * q + 1] = leaf(R, tR, par ^ t ^ tR);
+            if (++q == (nleaf >> 1)) break;
+            // next leaf parent: the right child stacked at depth d - 2 - ctz(q)
+            const uint32_t dp = d - 2 - ((uint32_t)__ffsll((long long)q) - 1);
+            const uint4    e  = stk[dp];
+            s[0] = e.x, s[1] = e.y, s[2] = e.z, s[3] = e.w;
+            t   = (tstk >> dp) & 1u;
+            par = (pstk >> dp) & 1u;
+            lv  = top + dp + 1;
         }
     }
 }
