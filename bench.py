@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the DPF, Grotto, batched and serving measurements")
     ap.add_argument("--sections", default="dpf,grotto,batched,serving",
                     help="comma-separated extra measurements to run after the DCF line")
+    ap.add_argument("--dpf-all-keys", type=int, default=1 << 12, help="keys of the full-domain DPF measurement")
     ap.add_argument("--batched-instances", type=int, default=256)
     ap.add_argument("--serving-requests", type=int, default=160)
     return ap.parse_args()
@@ -511,13 +512,14 @@ DPF_ALL_LOOKUPS_PER_KEY = ((1 << DPF_ALL_N) - 1) * 346 + (1 << DPF_ALL_N) * (40 
 
 
 def dpf_all_section(dev, args, peak_glookups) -> dict:
-    """Full-domain DPF evaluation (FastFss_cuda_dpfEvalAll): 2^12 keys at n = 16 over Z_2^32
-    (uint32), groupSize 1, every key expanded to its 2^16 outputs (1 GiB of shares per party)."""
+    """Full-domain DPF evaluation (FastFss_cuda_dpfEvalAll): 2^12 keys (--dpf-all-keys) at
+    n = 16 over Z_2^32 (uint32), groupSize 1, every key expanded to its 2^16 outputs (1 GiB of
+    shares per party at 2^12 keys)."""
     import torch
 
     import fastfunctionsecretsharing_b200 as F
 
-    n, N = DPF_ALL_N, 1 << 12
+    n, N = DPF_ALL_N, args.dpf_all_keys
     gen = torch.Generator(device=dev).manual_seed(8765)
     alpha = torch.randint(0, 1 << n, (N,), dtype=torch.int32, device=dev, generator=gen)
     beta = torch.randint(-2**31, 2**31, (N,), dtype=torch.int32, device=dev, generator=gen)
@@ -539,7 +541,7 @@ def dpf_all_section(dev, args, peak_glookups) -> dict:
     del alpha, beta, s0, s1, x, masked, key, y0, y1, want
     torch.cuda.empty_cache()
     ach = DPF_ALL_LOOKUPS_PER_KEY * N / (ms / 1e3) / 1e9
-    return {"workload": "full-domain DPF eval, 2^12 keys, n=16, Z_2^32 (uint32), groupSize 1, one party per step",
+    return {"workload": f"full-domain DPF eval, {N} keys, n=16, Z_2^32 (uint32), groupSize 1, one party per step",
             "keys": N, "kernel_ms": ms, "Gout_per_s": N * (1 << n) / (ms / 1e3) / 1e9,
             "out_gbs": out_bytes / (ms / 1e3) / 1e9,
             "roofline": {"bound": "smem", "achieved": ach, "peak": peak_glookups, "unit": "Glookup/s",
