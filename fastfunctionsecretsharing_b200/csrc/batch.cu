@@ -257,22 +257,29 @@ int batch_plan(const FastFssBatchOp *ops, size_t opNum, const FastFssBatchTuning
         rows.push_back({d, c});
         lookups += c * (double)items;
     }
-    // A batch too small to give every SM a full CTA of items is spread over all SMs instead:
-    // each op gets tiles in proportion to its share of the work, down to one warp of items (the
-    // CTAs then run partly idle, on SMs that would otherwise have nothing to do).
-    unsigned long long allItems = 0;
-    for (const auto &r : rows) allItems += r.d.items;
+    // Tile sizes by work. k = tiles per SM at the tuned tile cost (at least 1); every op gets
+    // tiles in proportion to its share of the work, so the batch splits into about k x SMs
+    // tiles of similar work that the atomic queue can balance. A tile holds whole CTAs of items
+    // when it is that large, else whole warps: a small batch then runs partly idle CTAs on SMs
+    // that would otherwise have nothing to do, instead of a few SMs working through large tiles.
+    // In a small batch (k = 1) no tile gives a thread more than one item: the ops' per-SM
+    // rates differ (a DCF element is one thread's serial walk, a spline element a warp's), so
+    // equal shares of lookups are not equal times; one-item tiles let the queue even them out.
     const unsigned long long sms = (unsigned long long)sm_count();
-    if (!rows.empty() && allItems < sms * threads && lookups > 0)
+    if (!rows.empty() && lookups > 0)
     {
+        const double k = std::max(1.0, std::floor(lookups / ((double)sms * tileCost)));
         for (auto &r : rows)
         {
-            const double share = r.cost * (double)r.d.items / lookups;
-            double       want  = std::ceil(share * (double)sms);
-            want               = want < 1 ? 1 : want;
-            unsigned long long ti = (unsigned long long)std::ceil((double)r.d.items / want);
-            ti                    = ((ti + 31) / 32) * 32;
-            r.d.tileItems         = std::min<unsigned long long>(r.d.tileItems, std::max<unsigned long long>(32, ti));
+            const double       share = r.cost * (double)r.d.items / lookups;
+            const double       want  = std::max(1.0, std::round(share * k * (double)sms));
+            unsigned long long ti    = (unsigned long long)std::ceil((double)r.d.items / want);
+            if (k == 1.0) ti = std::min<unsigned long long>(ti, threads);
+            if (ti >= threads)
+                ti = std::min<unsigned long long>((ti / threads) * threads, 1048576ull);
+            else
+                ti = std::max<unsigned long long>(32, ((ti + 31) / 32) * 32);
+            r.d.tileItems = ti;
         }
     }
     if (!callOrder)

@@ -12,9 +12,10 @@ as a Poisson process. The server
   persistent batched launch until the batch's estimated GPU time (algorithmic AES lookups at
   the lookup rate of the kernels) reaches `batch_cap_ms`, so early arrivals are not held back
   behind everything queued after them; a new batch is queued (on the stream slots in turn; one
-  slot by default, as every batch spans all SMs) while at most `max_inflight - 1` earlier
-  batches are still queued or running, so the device never idles between batches and a
-  request waits behind a bounded amount of work. Within a batch, requests that fill every SM
+  slot by default, as every batch spans all SMs) while the launches still queued or running
+  hold less than `max_inflight - 1` batches' worth of estimated GPU time, so the device never
+  idles between batches (a count of launches would let a queue that ends in a few tiny
+  launches drain) and a request waits behind a bounded amount of work. Within a batch, requests that fill every SM
   on their own (DCF requests of >= 148 x 512 elements, spline requests of >= 148 x 16) go out
   as their own per-call launches in queue order, and only the runs of smaller requests share a
   persistent batched launch (that is where one launch gains: small requests cannot fill the
@@ -213,7 +214,7 @@ class Server:
         self.dev = pools.dev
         self.store = KeyStore(capacity_bytes)
         self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
-        self.tuning = tuning or batch.Tuning(512, 1 << 26, 0, 0)
+        self.tuning = tuning  # None: per batch, see _tuning_for
         self.max_inflight = max(1, max_inflight)
         self.batch_cap = batch_cap_ms * 1e-3 * lookups_per_s
         self.launches = 0
@@ -236,7 +237,8 @@ class Server:
             for r in reqs:
                 self._plain_call(r, s)
             built = [self._build(r) for r in reqs]
-            batch.Batch(built, self.dev).prepare(self.tuning).launch()
+            batch.Batch(built, self.dev).prepare(self._tuning_for(reqs)).launch()
+            batch.Batch(built[:1], self.dev).prepare(batch.Tuning(512, 1 << 26, 0, 0)).launch()
         torch.cuda.synchronize(self.dev)
 
     def _build(self, r: Request) -> batch.Request:
@@ -295,6 +297,15 @@ class Server:
             if was:
                 gc.enable()
 
+    def _tuning_for(self, rs: list[Request]) -> batch.Tuning:
+        """The server's tuning if it was given one; otherwise 256-thread CTAs for a batch with
+        spline requests (the 512-thread persistent kernel must fit the spline path in 128
+        registers and spills) and 512-thread CTAs for DCF-only batches."""
+        if self.tuning is not None:
+            return self.tuning
+        threads = 256 if any(r.kind == "spline" for r in rs) else 512
+        return batch.Tuning(threads, 1 << 26, 0, 0)
+
     def _fills_gpu(self, r: Request) -> bool:
         """True if r's own launch already puts a full CTA on every SM (a DCF element is one
         thread, a spline element one warp)."""
@@ -314,7 +325,7 @@ class Server:
         h0 = time.perf_counter()
         with torch.cuda.stream(s):
             reqs = [self._build(r) for r in rs]
-            b = batch.Batch(reqs, self.dev).prepare(self.tuning)
+            b = batch.Batch(reqs, self.dev).prepare(self._tuning_for(rs))
             if self.batch_log is not None:
                 e0 = torch.cuda.Event(enable_timing=True)
                 e0.record(s)
@@ -337,7 +348,8 @@ class Server:
     def _run(self, requests: list[Request], mode: str, poll_s: float) -> float:
         pending: deque[Request] = deque()
         arrivals = deque(sorted(requests, key=lambda r: r.arrival))
-        inflight = []  # (event, slot index or None, [requests], keep-alive)
+        inflight = []  # (event, slot index or None, [requests], keep-alive, estimated lookups)
+        outstanding = 0  # estimated lookups of the launches in flight
         done, total = 0, len(requests)
         t0 = time.perf_counter()
         while done < total:
@@ -345,18 +357,19 @@ class Server:
             while arrivals and arrivals[0].arrival <= now:
                 pending.append(arrivals.popleft())
             still = []
-            for ev, si, rs, keep in inflight:
-                if ev.query():
+            for entry in inflight:
+                if entry[0].query():
                     tdone = time.perf_counter() - t0
-                    for r in rs:
+                    for r in entry[2]:
                         r.done = tdone
                         self.store.release(r.key_bytes)
-                    done += len(rs)
+                    done += len(entry[2])
+                    outstanding -= entry[4]
                 else:
-                    still.append((ev, si, rs, keep))
+                    still.append(entry)
             inflight = still
             if mode == "batched":
-                if pending and len(inflight) < self.max_inflight:
+                if pending and (not inflight or outstanding < (self.max_inflight - 1) * self.batch_cap):
                     admitted, cost = [], 0
                     while pending and (not admitted or cost + request_lookups(pending[0]) <= self.batch_cap) \
                             and self.store.try_admit(pending[0].key_bytes):
@@ -374,13 +387,18 @@ class Server:
                                 run.append(r)
                                 continue
                             if run:
-                                inflight.append(self._launch_batch(run, si, t0))
+                                cost = sum(request_lookups(q) for q in run)
+                                inflight.append((*self._launch_batch(run, si, t0), cost))
+                                outstanding += cost
                                 run = []
                             if r is not None:
-                                inflight.append(self._launch_plain(r, self.slots[si], t0))
+                                inflight.append((*self._launch_plain(r, self.slots[si], t0), request_lookups(r)))
+                                outstanding += request_lookups(r)
             else:
                 while pending and self.store.try_admit(pending[0].key_bytes):
-                    inflight.append(self._launch_plain(pending.popleft(), self.slots[0], t0))
+                    r = pending.popleft()
+                    inflight.append((*self._launch_plain(r, self.slots[0], t0), request_lookups(r)))
+                    outstanding += request_lookups(r)
             if not (arrivals and arrivals[0].arrival <= time.perf_counter() - t0):
                 time.sleep(poll_s)
         return time.perf_counter() - t0
