@@ -169,8 +169,9 @@ static double item_cost(const FastFssBatchOp &o, uint32_t G)
         case FAST_FSS_BATCH_DCF_MIC_EVAL: return 2.0 * n * 340.0;
         case FAST_FSS_BATCH_SPLINE_EVAL:
         {
-            const double per_q = ((double)o.intervalNum + G - 1) / G;
-            const double chunks = ((double)o.degree + 1 + kSplineMaxC - 1) / kSplineMaxC;
+            // whole passes: interval groups per lane and coefficient chunks per slot
+            const double per_q  = (double)((o.intervalNum + G - 1) / G);
+            const double chunks = (double)((o.degree + 1 + kSplineMaxC - 1) / kSplineMaxC);
             return per_q * chunks * 2.0 * n * (340.0 + 360.0);
         }
         case FAST_FSS_BATCH_GROTTO_EVAL: return (n - 6) * 200.0;
