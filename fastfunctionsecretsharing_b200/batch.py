@@ -111,16 +111,28 @@ def grotto_request(out, maskedX, key, seed, equalBound, partyId, bitWidthIn) -> 
     return Request(op, [out, maskedX, key, seed], maskedX.numel())
 
 
+def workspace_size(opNum: int) -> int:
+    """Device bytes a batch of opNum ops needs (FastFss_cuda_batchWorkspaceSize)."""
+    return int(_fn("FastFss_cuda_batchWorkspaceSize")(opNum))
+
+
 class Batch:
     """A fixed set of requests, prepared once and launched any number of times."""
 
-    def __init__(self, requests: list[Request], device: torch.device | str = "cuda"):
+    def __init__(self, requests: list[Request], device: torch.device | str = "cuda",
+                 workspace: torch.Tensor | None = None):
+        """`workspace`: a device byte buffer to hold the queue counter and op table instead of a
+        fresh allocation (at least workspace_size(len(requests)) bytes). Batches that share one
+        must run on one stream, where each launch finishes before the next prepare's copy."""
         self.requests = list(requests)
         self.device = torch.device(device)
         self.ops = (BatchOp * max(1, len(self.requests)))(*[r.op for r in self.requests])
         n = len(self.requests)
-        ws = int(_fn("FastFss_cuda_batchWorkspaceSize")(n))
-        self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
+        ws = workspace_size(n)
+        if workspace is not None and workspace.numel() >= ws:
+            self.workspace = workspace
+        else:
+            self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
         self.plan = Plan()
         self.tuning = Tuning(256, 1 << 26, 0, 0)
         self.elements = sum(r.elements for r in self.requests)

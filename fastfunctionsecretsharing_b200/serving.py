@@ -208,12 +208,17 @@ def request_lookups(r: Request) -> int:
 
 
 class Server:
+    MAX_BATCH_OPS = 4096  # requests per batch that fit the preallocated workspace
     def __init__(self, pools: Pools, capacity_bytes=64 << 30, slots=1, tuning: batch.Tuning | None = None,
                  max_inflight: int = 2, batch_cap_ms: float = 4.0, lookups_per_s: float = 8.0e12):
         self.P = pools
         self.dev = pools.dev
         self.store = KeyStore(capacity_bytes)
         self.slots = [torch.cuda.Stream(self.dev) for _ in range(slots)]
+        # one batch workspace per stream slot (batches on a slot run in order), so serving
+        # allocates nothing per batch
+        self.workspaces = [torch.empty(batch.workspace_size(self.MAX_BATCH_OPS), dtype=torch.uint8, device=self.dev)
+                           for _ in range(slots)]
         self.tuning = tuning  # None: per batch, see _tuning_for
         self.max_inflight = max(1, max_inflight)
         self.batch_cap = batch_cap_ms * 1e-3 * lookups_per_s
@@ -325,7 +330,7 @@ class Server:
         h0 = time.perf_counter()
         with torch.cuda.stream(s):
             reqs = [self._build(r) for r in rs]
-            b = batch.Batch(reqs, self.dev).prepare(self._tuning_for(rs))
+            b = batch.Batch(reqs, self.dev, workspace=self.workspaces[si]).prepare(self._tuning_for(rs))
             if self.batch_log is not None:
                 e0 = torch.cuda.Event(enable_timing=True)
                 e0.record(s)
