@@ -353,6 +353,7 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
     const size_t   work  = N * S;
     const size_t   words = (size_t)1 << D; // leaf words per key
     const size_t   nleaf = (size_t)1 << d;
+    const bool     vec   = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
     for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += (size_t)gridDim.x * blockDim.x)
     {
         const size_t      i = w >> top, sub = w & (S - 1);
@@ -407,8 +408,12 @@ __global__ void __launch_bounds__(kGrottoThreads, 1)
                 lv++;
                 continue;
             }
-            row[2 * q]     = leaf(L, tL, par);
-            row[2 * q + 1] = leaf(R, tR, par ^ t ^ tR);
+            // the two leaf words are adjacent: one 16-byte store when the rows are 16-byte aligned
+            const unsigned long long wl = leaf(L, tL, par), wr = leaf(R, tR, par ^ t ^ tR);
+            if (vec)
+                reinterpret_cast<ulonglong2 *>(row)[q] = make_ulonglong2(wl, wr);
+            else
+                row[2 * q] = wl, row[2 * q + 1] = wr;
             if (++q == (nleaf >> 1)) break;
             // next leaf parent: the right child stacked at depth d - 2 - ctz(q)
             const uint32_t dp = d - 2 - ((uint32_t)__ffsll((long long)q) - 1);

@@ -134,6 +134,24 @@ def test_full_domain_vs_oracle(F, oracle, es, n):
         assert np.array_equal(host(le), oracle.grotto_le_eval_all(kref, s, p, n, es, N))
 
 
+@pytest.mark.parametrize("n", [7, 13])
+def test_full_domain_rows_at_8_byte_offset(F, oracle, n):
+    """Rows written to a buffer that is 8- but not 16-byte aligned (word-by-word stores) equal
+    the oracle's, as do rows in an aligned buffer (paired 16-byte stores)."""
+    rng = np.random.default_rng(n)
+    N, es = 5, 2
+    a, s0, s1 = rnd(rng, N, es, n), seeds(rng, N), seeds(rng, N)
+    kref = oracle.grotto_keygen(a, s0, s1, n)
+    nbytes = N * (1 << n) // 8
+    for op, ref in ((F.grotto_eq_eval_all, oracle.grotto_eq_eval_all), (F.grotto_le_eval_all, oracle.grotto_le_eval_all)):
+        buf = torch.zeros(nbytes + 16, dtype=torch.uint8, device="cuda")
+        view = buf[8:8 + nbytes]
+        assert view.data_ptr() % 16 == 8
+        op(view, dev_bytes(kref), dev_bytes(s1), 1, n, es, N)
+        assert np.array_equal(host(view), ref(kref, s1, 1, n, es, N))
+        assert not host(buf[:8]).any() and not host(buf[8 + nbytes:]).any()
+
+
 def test_full_domain_config3_reconstruction(F):
     """BASELINE config 3 size: 2^16 keys at n = 16, full domain. Party rows XOR to the one-hot
     of alpha (eq) and to the prefix [x <= alpha] (le) for every key (checked on the device)."""
