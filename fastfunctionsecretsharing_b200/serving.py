@@ -13,9 +13,10 @@ as a Poisson process. The server
   the lookup rate of the kernels) reaches `batch_cap_ms`, so early arrivals are not held back
   behind everything queued after them; a new batch is queued (on the stream slots in turn; one
   slot by default, as every batch spans all SMs) while the launches still queued or running
-  hold less than `max_inflight - 1` batches' worth of estimated GPU time, so the device never
-  idles between batches (a count of launches would let a queue that ends in a few tiny
-  launches drain) and a request waits behind a bounded amount of work. Within a batch, requests that fill every SM
+  hold less than `max_inflight` batches' worth of estimated GPU time (a launch counts in full
+  until it completes, so the next round is queued behind a long launch instead of after it),
+  so the device never idles between batches (a count of launches would let a queue that ends
+  in a few tiny launches drain) and a request waits behind a bounded amount of work. Within a batch, requests that fill every SM
   on their own (DCF requests of >= 148 x 512 elements, spline requests of >= 148 x 16) go out
   as their own per-call launches in queue order, and only the runs of smaller requests share a
   persistent batched launch (that is where one launch gains: small requests cannot fill the
@@ -374,7 +375,7 @@ class Server:
                     still.append(entry)
             inflight = still
             if mode == "batched":
-                if pending and (not inflight or outstanding < (self.max_inflight - 1) * self.batch_cap):
+                if pending and (not inflight or outstanding < self.max_inflight * self.batch_cap):
                     admitted, cost = [], 0
                     while pending and (not admitted or cost + request_lookups(pending[0]) <= self.batch_cap) \
                             and self.store.try_admit(pending[0].key_bytes):
