@@ -675,7 +675,7 @@ def serving_section(dev, args) -> dict:
     out = {"workload": ("12-layer MLP (width 4096, batch 64) trace: 2^18 ReLU DCFs (n=32) + 2^18 GeLU splines "
                         "(n=64, 32 intervals, degree 2) per layer, issued as requests of 2^k elements (DCF k in "
                         "10..20, spline k in 10..14); key store 64 GB charged per request; batches capped at about "
-                        "4 ms of GPU work, a new batch queued while under one batch of estimated work is in flight on "
+                        "4 ms of GPU work, a new batch queued while under two batches of estimated work are in flight on "
                         "one stream; plain = one per-call C-ABI "
                         "evaluation per request, FIFO on one stream"),
            "rates": []}
