@@ -91,6 +91,25 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
     }
 }
 
+// One leaf's g outputs. With groupSize 1 (G1) the convert (init(seed, bitWidthOut, 1), values
+// of one byte) yields byte 0 of its stream: byte 0 of the seed when bitWidthOut <= 16, else
+// byte 0 of AES_seed(0^128).
+template <typename GE, bool G1>
+__device__ __forceinline__ void dpf_all_leaf(const AesLanes &A, GE *o, const uint32_t s[4], uint32_t t, const GE *kb,
+                                             uint64_t last, uint32_t party, uint32_t bo, uint32_t g)
+{
+    if constexpr (G1)
+    {
+        const uint32_t b = (bo <= 16) ? (s[0] >> 24) : (aes_zero_block_word0(A, s) >> 24);
+        const uint64_t v = (uint64_t)b + (t ? last : 0);
+        o[0]             = (GE)(party ? (0 - v) : v);
+    }
+    else
+    {
+        dpf_leaf<GE>(A, o, s, t, kb, party, bo, g);
+    }
+}
+
 // Multi-point evaluation (work = N P): point j of element i evaluates at maskedX - point[j]
 // (src/kernel/dpf.h:490-495), one tree walk per (element, point).
 template <typename GE>
@@ -121,25 +140,6 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
 // children wait on a stack (16-byte entries, control bits in a register). An element costs
 // 2^n - 1 node expansions plus 2^n leaf converts instead of n 2^n single-child steps.
 constexpr uint32_t kDpfAllMaxSub = 8;
-
-// One leaf's g outputs. With groupSize 1 (G1) the convert (init(seed, bitWidthOut, 1), values
-// of one byte) yields byte 0 of its stream: byte 0 of the seed when bitWidthOut <= 16, else
-// byte 0 of AES_seed(0^128).
-template <typename GE, bool G1>
-__device__ __forceinline__ void dpf_all_leaf(const AesLanes &A, GE *o, const uint32_t s[4], uint32_t t, const GE *kb,
-                                             uint64_t last, uint32_t party, uint32_t bo, uint32_t g)
-{
-    if constexpr (G1)
-    {
-        const uint32_t b = (bo <= 16) ? (s[0] >> 24) : (aes_zero_block_word0(A, s) >> 24);
-        const uint64_t v = (uint64_t)b + (t ? last : 0);
-        o[0]             = (GE)(party ? (0 - v) : v);
-    }
-    else
-    {
-        dpf_leaf<GE>(A, o, s, t, kb, party, bo, g);
-    }
-}
 
 // The loop has a single call site for the node expansion and one for the leaf convert, so
 // the kernel's code stays small; the n - d levels above the subtree also expand both
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
 // copy does not arrive in time counts the failure in g_dpf_stage_failures, drains and stops.
 __device__ unsigned int g_dpf_stage_failures;
 
-template <typename GE>
+template <typename GE, bool G1>
 __global__ void __launch_bounds__(kDpfThreads, 1)
     dpf_eval_staged_kernel(GE *__restrict__ out, const GE *__restrict__ maskedX, const uint8_t *__restrict__ key,
                            const uint8_t *__restrict__ seed, uint32_t party, uint32_t n, uint32_t bo, uint32_t g,
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kDpfThreads, 1)
             S.next();
         }
         if (failed) break;
-        if (active) dpf_leaf<GE>(A, out + i * g, s, t, kb, party, bo, g);
+        if (active) dpf_all_leaf<GE, G1>(A, out + i * g, s, t, kb, (uint64_t)__ldg(kb + 2), party, bo, g);
     }
     if (failed)
     {
@@ -328,7 +328,7 @@ static int dpf_launch(void *out, const void *maskedX, const void *key, const voi
     {
         CUtensorMap map;
         if (!encode_region_a_map(&map, key, n, N)) return FAST_FSS_RUNTIME_ERROR;
-        auto           kern    = dpf_eval_staged_kernel<GE>;
+        auto           kern    = (g == 1) ? dpf_eval_staged_kernel<GE, true> : dpf_eval_staged_kernel<GE, false>;
         const int      threads = aes_threads(N, kDpfThreads);
         if (!ensure_smem(reinterpret_cast<const void *>(kern), stage_smem_bytes(kDpfThreads / 32)))
             return FAST_FSS_RUNTIME_ERROR;
